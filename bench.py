@@ -1,0 +1,313 @@
+"""Benchmark of the wavefront path tracer on the 262,144-triangle scene (1920x1080, 16 spp, max depth 12).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step renders one full frame (1920 x 1080 x 16 = 33,177,600 paths) through pt_render on a scene
+already resident in device memory; the metric is Msamples/s (a sample is one whole path). Steps are
+timed on the device with CUDA events recorded on the renderer's own stream, one event pair per
+step, with a 256 MiB write between steps to flush the 126 MB L2; the JSON line reports the whole
+job (all ranks) and max-over-ranks time. Under torchrun each rank renders its own frames (weak
+scaling, replicas: no collective on the data path).
+
+Also reported: `e2e` (pt_render + pt_download_image into a host buffer, wall clock per step), the
+roofline of the dominant kernel from the library's per-kernel event timing and traversal counters,
+clocks sampled with nvidia-smi during the timed region, and the reference CPU renderer timed on the
+host cores on a bounded sample. `--impl reference` times only the reference CPU path.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Msamples/s at 262K tris; p50/p99 request latency, served vs plain, 1 B200"
+UNIT = "Msamples/s"
+WIDTH, HEIGHT, SPP, DEPTH, TRIS, SEED = 1920, 1080, 16, 12, 262144, 1
+WORKLOAD = "262,144-triangle terrain scene (value-noise height field + 200 instanced shapes, 64 materials, " \
+           "64 emitters, 4 punctual lights, 1024x512 HDR sky), 1920x1080, 16 spp, max depth 12, seed 1"
+# Algorithmic bytes of the traversal kernels: one 64-byte node per visit, one 48-byte triangle per test.
+NODE_BYTES, TRI_BYTES = 64, 48
+
+
+def dist_info():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def init_dist(world, local):
+    if world <= 1:
+        return None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return dist
+
+
+def reduce_max(dist, value, local):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi samples (every 200 ms) of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(desc, cam, seconds_hint=20.0):
+    """Photon's own CpuRenderer (oracle/_ref, built from its sources) on all host cores, on a bounded
+    sample: 1 spp of the full 1920x1080 frame after a 1 spp warm-up at 480x270."""
+    from oracle import oracle as O
+    from photon_b200 import abi
+    if not O.reference_available():
+        return None
+    ref = O.RefScene.from_desc(desc)
+    cores = os.cpu_count() or 1
+    warm = abi.render_settings(480, 270, max_depth=DEPTH, seed=SEED)
+    ref.render(cam, warm, 1, threads=cores)
+    rs = abi.render_settings(WIDTH, HEIGHT, max_depth=DEPTH, seed=SEED)
+    _, secs = ref.render(cam, rs, 1, threads=cores)
+    return {"value": WIDTH * HEIGHT / secs / 1e6, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"1 spp of the 1920x1080 frame ({WIDTH * HEIGHT} paths, {secs:.2f} s) after a 1 spp 480x270 warm-up"}
+
+
+def run_reference(args, world, rank):
+    """The reference arm: Photon's own CPU renderer on the host cores (rank 0 only)."""
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    from photon_b200 import abi, native
+    if not O.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "Photon's CPU build (oracle/_ref/libphoton_ref.so) is missing"}))
+        return 0
+    g = native.terrain_scene(TRIS, SEED)
+    b = g.build()
+    cam = g.camera(WIDTH / HEIGHT)
+    ref = O.RefScene.from_desc(b.desc)
+    cores = os.cpu_count() or 1
+    # Each step: 1 spp over a 960x540 window of the frame's camera (a bounded sample of the workload).
+    w, h = 960, 540
+    rs = abi.render_settings(w, h, max_depth=DEPTH, seed=SEED)
+    for _ in range(args.warmup):
+        ref.render(cam, rs, 1, threads=cores)
+    t = []
+    for _ in range(args.steps):
+        _, secs = ref.render(cam, rs, 1, threads=cores)
+        t.append(secs)
+    total = sum(t)
+    value = args.steps * w * h / total / 1e6
+    sample = f"1 spp of a 960x540 image of the same scene and camera per step ({w * h} paths), all {cores} host threads"
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural scene, seeded)",
+            "config": {"workload": WORKLOAD, "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_info()
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+    if args.warmup < 3:
+        args.warmup = 3
+
+    import torch
+    from photon_b200 import abi, native
+
+    dist = init_dist(world, local)
+    torch.cuda.set_device(local)
+    g = native.terrain_scene(TRIS, SEED)
+    b = g.build()
+    desc = b.desc
+    cam = g.camera(WIDTH / HEIGHT)
+    rs = abi.render_settings(WIDTH, HEIGHT, max_depth=DEPTH, seed=SEED + rank)
+    r = native.Renderer(local)
+    r.upload(desc)
+    r.resize(WIDTH, HEIGHT)
+    stream = torch.cuda.ExternalStream(r.stream(), device=f"cuda:{local}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    # Warm-up, then one untimed render with traversal counters (the roofline's algorithmic bytes).
+    for _ in range(args.warmup):
+        r.render(cam, rs, SPP)
+        r.reset()
+    r.set_profiling(abi.PT_PROFILE_TRAVERSAL_COUNTS)
+    r.render(cam, rs, SPP)
+    r.reset()
+    counts = r.profile()
+
+    # Timed steps.
+    r.set_profiling(abi.PT_PROFILE_KERNEL_TIMES)
+    clocks = ClockSampler(local)
+    barrier(dist)
+    torch.cuda.synchronize()
+    clocks.start()
+    step_ms = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+        r.render(cam, rs, SPP)
+        end.record(stream)
+        end.synchronize()
+        step_ms.append(start.elapsed_time(end))
+        r.reset()
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    barrier(dist)
+    prof = r.profile()
+    total_ms = reduce_max(dist, float(sum(step_ms)), local)
+    samples_per_step = WIDTH * HEIGHT * SPP
+    value = world * args.steps * samples_per_step / (total_ms / 1000.0) / 1e6
+
+    # End to end through the C ABI: render + download into a host buffer, wall clock.
+    e2e_t = []
+    host = np.zeros((HEIGHT, WIDTH, 3), np.float32)
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r.reset()
+        r.render(cam, rs, SPP)
+        img = r.download_image()
+        e2e_t.append(time.perf_counter() - t0)
+    host[...] = img
+    e2e_total = reduce_max(dist, float(sum(e2e_t)), local)
+    e2e_value = world * args.steps * samples_per_step / e2e_total / 1e6
+
+    # Roofline of the dominant kernel.
+    kernels = {"setup": prof.setup.ms, "generate": prof.generate.ms, "trace": prof.trace.ms, "shade": prof.shade.ms,
+               "shadow": prof.shadow.ms, "accumulate": prof.accumulate.ms}
+    ktotal = sum(kernels.values()) or 1.0
+    trace_bytes_per_frame = counts.closest_node_visits * NODE_BYTES + counts.closest_tri_tests * TRI_BYTES
+    shadow_bytes_per_frame = counts.shadow_node_visits * NODE_BYTES + counts.shadow_tri_tests * TRI_BYTES
+    peak, peak_kind = measured_peak()
+    trace_launches = max(1, prof.trace.launches)
+    achieved = (trace_bytes_per_frame * args.steps) / (prof.trace.ms / 1000.0) / 1e9 if prof.trace.ms > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": "k_trace (closest-hit BVH traversal)", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+                "traffic": None,
+                "algorithmic_bytes_per_launch": trace_bytes_per_frame * args.steps / trace_launches,
+                "avg_launch_ms": prof.trace.ms / trace_launches,
+                "model": "64 B per node visit + 48 B per triangle test (closest-hit rays)",
+                "node_visits_per_ray": counts.closest_node_visits / max(1, counts.closest_rays),
+                "tri_tests_per_ray": counts.closest_tri_tests / max(1, counts.closest_rays),
+                "shadow_bytes_per_frame": shadow_bytes_per_frame}
+    rays_per_sample = (counts.closest_rays + counts.shadow_rays) / samples_per_step
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (procedural scene, seeded; no dataset)",
+            "config": {"workload": WORKLOAD, "scene_triangles": desc.num_tris, "width": WIDTH, "height": HEIGHT,
+                       "spp": SPP, "max_depth": DEPTH, "samples_per_step": samples_per_step,
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": "flushed between steps (256 MiB write, outside the event pair)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 64 + 36 + 256,
+                    "d2h_bytes_per_step": WIDTH * HEIGHT * 16, "api": "pt_reset + pt_render + pt_download_image"},
+            "gpu_launches": prof.kernel_launches,
+            "rays_per_sample": rays_per_sample,
+            "mrays_per_s": value * rays_per_sample,
+            "kernel_ms_per_step": {k: v / args.steps for k, v in kernels.items()},
+            "kernel_share": {k: v / ktotal for k, v in kernels.items()},
+            "roofline": roofline,
+            "clocks": clock_info}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(desc, cam)
+    if rank == 0:
+        print(json.dumps(line))
+    del stream
+    r.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

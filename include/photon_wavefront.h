@@ -1,0 +1,405 @@
+/*
+ * photon_wavefront.h — the C ABI of the B200 wavefront path tracer.
+ *
+ * This is the drop-in boundary for Photon's GPU renderer. Every entry point below replaces one member
+ * of photon::GpuRenderer (src/render/gpu_renderer.h:36-75 of the Photon sources) or one of the
+ * systems forms built beside it (batched views, the request server, SVGF on caller G-buffers).
+ *
+ * Conventions
+ *  - Plain C: opaque handles, plain pointers and sizes, int status codes (PT_OK = 0). The message of
+ *    the last failure on a handle is returned by pt_last_error(handle); pt_global_error() holds the
+ *    message of failures that happen before a handle exists.
+ *  - Scene arrays are COPIED at upload; the caller keeps ownership of every pointer it passes.
+ *  - The POD types below have exactly the byte layout of the Photon types named beside them
+ *    (src/render/scene_view.h:13-150, src/render/pixel.h:10-16, src/render/integrator.h:21-27), so a
+ *    built photon::Scene is passed by pointer casts, without repacking.
+ *  - Image buffers are row-major, pixel (x, y) at index y * width + x, RGB float triples unless said.
+ *  - A renderer handle is used from one host thread at a time (as GpuRenderer). The server handle is
+ *    thread-safe: pt_server_submit / poll / wait / fetch / cancel may be called from any thread.
+ */
+#ifndef PHOTON_WAVEFRONT_H
+#define PHOTON_WAVEFRONT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PT_ABI_VERSION 1
+
+/* ---- status codes -------------------------------------------------------------------------- */
+enum {
+    PT_OK = 0,
+    PT_ERR_INVALID = -1,     /* a null handle, a bad size, an inconsistent scene description */
+    PT_ERR_CUDA = -2,        /* a CUDA call failed; the message names it */
+    PT_ERR_NO_DEVICE = -3,   /* no CUDA device, or not an sm_100 device */
+    PT_ERR_NO_SCENE = -4,    /* render before upload */
+    PT_ERR_BUDGET = -5,      /* the request or scene does not fit the device-memory budget */
+    PT_ERR_TIMEOUT = -6,     /* a wait ran out of time (host wait or a bounded device wait) */
+    PT_ERR_CANCELLED = -7,   /* the request was cancelled */
+    PT_ERR_NOT_FOUND = -8,   /* unknown request or scene id */
+    PT_ERR_OVERFLOW = -9,    /* a device queue overflowed (counted on the device, never trapped) */
+    PT_ERR_ALLOC = -10       /* a host or device allocation failed */
+};
+
+/* ---- POD types with Photon's layouts ------------------------------------------------------- */
+typedef struct pt_vec2 { float x, y; } pt_vec2;
+typedef struct pt_vec3 { float x, y, z; } pt_vec3;
+typedef struct pt_vec4 { float x, y, z, w; } pt_vec4;
+
+/* photon::BvhNode (scene_view.h:13-22), 64 bytes: the boxes of both children. A child with
+ * count > 0 is a leaf over triangles [index, index + count) in BVH order; otherwise index is the
+ * child node (or -1 for an empty child). */
+typedef struct pt_bvh_node {
+    pt_vec3 lmin; int32_t left;
+    pt_vec3 lmax; int32_t lcount;
+    pt_vec3 rmin; int32_t right;
+    pt_vec3 rmax; int32_t rcount;
+} pt_bvh_node;
+
+/* photon::TriGeom (scene_view.h:25-32), 48 bytes: a vertex and two edges, in BVH order. */
+typedef struct pt_tri_geom {
+    pt_vec3 v0; int32_t material;
+    pt_vec3 e1; int32_t flags;   /* PT_TRI_ALPHA_TESTED */
+    pt_vec3 e2; int32_t pad;
+} pt_tri_geom;
+#define PT_TRI_ALPHA_TESTED 1
+
+/* photon::TextureInfo (scene_view.h:38-44). */
+typedef struct pt_texture_info {
+    int32_t width, height;
+    uint32_t offset;      /* into the RGBA8 texel pool */
+    int32_t wrap_repeat;  /* 1 repeat, 0 clamp */
+    int32_t srgb;
+} pt_texture_info;
+
+enum { PT_ALPHA_OPAQUE = 0, PT_ALPHA_MASK = 1, PT_ALPHA_BLEND = 2 };
+
+/* photon::Material (scene_view.h:46-63), 80 bytes. */
+typedef struct pt_material {
+    pt_vec4 base_color;
+    pt_vec3 emission;
+    float metallic, roughness, ior, transmission, normal_scale, alpha_cutoff;
+    int32_t alpha_mode, double_sided;
+    int32_t base_color_tex, metallic_roughness_tex, normal_tex, emissive_tex, occlusion_tex;
+} pt_material;
+
+/* photon::EmissiveTri (scene_view.h:65-69) and photon::AliasEntry (:71-76). */
+typedef struct pt_emissive_tri { int32_t tri; float area; } pt_emissive_tri;
+typedef struct pt_alias_entry { float prob; int32_t alias; float pmf; int32_t pad; } pt_alias_entry;
+
+enum { PT_LIGHT_POINT = 0, PT_LIGHT_SPOT = 1, PT_LIGHT_DIRECTIONAL = 2 };
+
+/* photon::PunctualLight (scene_view.h:81-88), 48 bytes. */
+typedef struct pt_punctual_light {
+    pt_vec3 position; int32_t type;
+    pt_vec3 direction; float cos_inner;
+    pt_vec3 intensity; float cos_outer;
+} pt_punctual_light;
+
+/* photon::CameraView (scene_view.h:106-115), 64 bytes. */
+typedef struct pt_camera {
+    pt_vec3 position; float tan_half_fov;
+    pt_vec3 forward; float aspect;
+    pt_vec3 right; float aperture;
+    pt_vec3 up; float focus_distance;
+} pt_camera;
+
+/* photon::PathOptions (integrator.h:21-27) without the host-only ray counter. */
+typedef struct pt_path_options {
+    int32_t max_depth;   /* path vertices after the camera (Photon default 8) */
+    int32_t rr_depth;    /* Russian roulette from this many bounces (3) */
+    float clamp;         /* luminance clamp of indirect light, 0 = off */
+    int32_t nee;         /* next event estimation on/off (1) */
+} pt_path_options;
+
+enum { PT_TONEMAP_LINEAR = 0, PT_TONEMAP_ACES = 1, PT_TONEMAP_REINHARD = 2 };
+
+/* photon::RenderSettings (pixel.h:10-16). */
+typedef struct pt_render_settings {
+    int32_t width, height;
+    pt_path_options path;
+    float exposure;
+    int32_t tonemap;
+    uint32_t seed;
+} pt_render_settings;
+
+/* photon::SvgfSettings (gpu_renderer.h:18-25). */
+typedef struct pt_svgf_settings {
+    int32_t atrous_iterations;
+    float alpha_color, alpha_moments, phi_color, phi_normal, phi_depth;
+} pt_svgf_settings;
+
+/* photon::DisplayMode (gpu_renderer.h:16). */
+enum { PT_DISPLAY_COLOR = 0, PT_DISPLAY_ALBEDO = 1, PT_DISPLAY_NORMAL = 2, PT_DISPLAY_DEPTH = 3,
+       PT_DISPLAY_VARIANCE = 4, PT_DISPLAY_HEATMAP = 5 };
+
+/* A built scene: the arrays photon::Scene::build produces (scene.h:75-89) and the scalars of
+ * photon::SceneView (scene_view.h:117-150). Optional arrays may be NULL with a zero count. */
+typedef struct pt_scene_desc {
+    const pt_bvh_node* nodes; int32_t num_nodes;
+    const pt_tri_geom* tris; int32_t num_tris;      /* BVH order */
+    const int32_t* indices;                          /* 3 * num_tris vertex indices, BVH order */
+    const pt_vec3* normals;                          /* num_vertices or NULL */
+    const pt_vec2* uvs;                              /* num_vertices or NULL */
+    const pt_vec4* tangents;                         /* num_vertices or NULL */
+    int32_t num_vertices;
+    const pt_material* materials; int32_t num_materials;
+    const pt_texture_info* textures; int32_t num_textures;
+    const uint32_t* texels; uint64_t num_texels;     /* RGBA8 pool */
+    const float* srgb_lut;                           /* 256 entries */
+    const pt_emissive_tri* emissive; int32_t num_emissive;
+    const int32_t* tri_emissive;                     /* num_tris entries (index into emissive or -1) */
+    const pt_alias_entry* emissive_alias;            /* num_emissive entries */
+    float emissive_power;
+    const pt_punctual_light* punctual; int32_t num_punctual;
+    const pt_vec3* env_texels; int32_t env_width, env_height;
+    const float* env_marginal;                       /* env_height + 1 */
+    const float* env_conditional;                    /* env_height * (env_width + 1) */
+    float env_intensity, env_rotation;
+    pt_vec3 env_color;
+    float env_integral;
+    float p_env, p_emissive, p_punctual;
+    pt_vec3 bounds_min, bounds_max;
+} pt_scene_desc;
+
+/* ---- library ------------------------------------------------------------------------------- */
+
+/* The ABI version compiled into the library (PT_ABI_VERSION). */
+int32_t pt_abi_version(void);
+/* photon::cuda_available (gpu_renderer.h:34): 1 with a usable device, else 0. Fills the
+ * optional outputs (name up to name_len bytes, compute capability, memory, SM count). */
+int32_t pt_device_info(char* name, size_t name_len, int32_t* major, int32_t* minor, uint64_t* memory_bytes,
+                       int32_t* multiprocessors);
+/* The message of the last failure that had no handle to attach to. */
+const char* pt_global_error(void);
+
+/* ---- plain renderer: photon::GpuRenderer ------------------------------------------------------ */
+typedef struct pt_renderer pt_renderer;
+
+/* GpuRenderer::GpuRenderer (gpu_renderer.h:38). device = CUDA ordinal. */
+int32_t pt_create(int32_t device, pt_renderer** out);
+/* GpuRenderer::~GpuRenderer (gpu_renderer.h:39). NULL is accepted. */
+void pt_destroy(pt_renderer* r);
+/* The message of the last failed call on r (empty when none). */
+const char* pt_last_error(const pt_renderer* r);
+
+/* GpuRenderer::upload (gpu_renderer.h:44, gpu_renderer.cu:243-297): copies the built scene to the
+ * device (re-laid for 128-bit loads) and resets the accumulation. */
+int32_t pt_upload_scene(pt_renderer* r, const pt_scene_desc* scene);
+/* GpuRenderer::update_lights (gpu_renderer.h:46, gpu_renderer.cu:299-334): re-uploads triangles,
+ * materials, light tables and the environment of a scene whose BVH is unchanged. */
+int32_t pt_update_lights(pt_renderer* r, const pt_scene_desc* scene);
+/* GpuRenderer::resize (gpu_renderer.h:47, gpu_renderer.cu:336-351). */
+int32_t pt_resize(pt_renderer* r, int32_t width, int32_t height);
+/* GpuRenderer::reset (gpu_renderer.h:48, gpu_renderer.cu:353-360). */
+int32_t pt_reset(pt_renderer* r);
+/* GpuRenderer::render (gpu_renderer.h:51, gpu_renderer.cu:362-377): adds spp samples per pixel. */
+int32_t pt_render(pt_renderer* r, const pt_camera* camera, const pt_render_settings* settings, int32_t spp);
+/* GpuRenderer::render_denoised (gpu_renderer.h:53, gpu_renderer.cu:379-401): one sample per pixel
+ * with the full G-buffer, denoised by SVGF against the previous camera. */
+int32_t pt_render_denoised(pt_renderer* r, const pt_camera* camera, const pt_camera* previous,
+                           const pt_render_settings* settings, const pt_svgf_settings* svgf);
+/* GpuRenderer::display (gpu_renderer.h:56, gpu_renderer.cu:403-426): tone maps into the RGBA8
+ * display buffer, or into device_target (caller-owned device memory, width*height words). */
+int32_t pt_display(pt_renderer* r, const pt_render_settings* settings, int32_t mode, uint32_t* device_target);
+/* GpuRenderer::download_image (gpu_renderer.h:58, gpu_renderer.cu:428-443): the average radiance,
+ * 3 floats per pixel, into rgb (capacity n floats). */
+int32_t pt_download_image(pt_renderer* r, float* rgb, size_t n);
+/* GpuRenderer::download_display (gpu_renderer.h:59): n words. */
+int32_t pt_download_display(pt_renderer* r, uint32_t* rgba8, size_t n);
+/* The G-buffer of the first sample of the last pt_render (or of the last pt_render_denoised):
+ * albedo (4 floats/pixel) and normal + depth (4 floats/pixel). Either pointer may be NULL. */
+int32_t pt_download_gbuffer(pt_renderer* r, float* albedo4, float* normal_depth4, size_t n_pixels);
+/* GpuRenderer::display_buffer (gpu_renderer.h:65): the device address of the RGBA8 buffer. */
+uint32_t* pt_display_buffer(pt_renderer* r);
+
+typedef struct pt_stats {
+    int32_t width, height, samples;
+    float last_frame_ms;          /* GpuRenderer::last_frame_ms (gpu_renderer.h:64) */
+    uint64_t paths;               /* paths traced by the last render */
+    uint64_t rays;                /* camera + extension + shadow rays of the last render */
+    uint64_t shadow_rays;
+    uint64_t bounce_iterations;   /* wavefront iterations of the last render */
+    uint64_t queue_overflows;     /* must stay 0 */
+    uint64_t device_bytes;        /* device memory held by this renderer */
+} pt_stats;
+/* Accessors width/height/samples/last_frame_ms (gpu_renderer.h:61-64) plus wavefront counters. */
+int32_t pt_get_stats(const pt_renderer* r, pt_stats* out);
+
+/* Tuning of the wavefront (the autotuner's knobs). Zero fields keep the current value. */
+typedef struct pt_tuning {
+    int32_t path_capacity;     /* paths in flight */
+    int32_t trace_block;       /* threads per block of the traversal kernels */
+    int32_t shade_block;       /* threads per block of the shading kernel */
+    int32_t sort_by_material;  /* 1: shade in material order, 0: in queue order, -1: keep */
+    int32_t graph_bounces;     /* bounce iterations captured per CUDA graph launch */
+} pt_tuning;
+int32_t pt_set_tuning(pt_renderer* r, const pt_tuning* t);
+int32_t pt_get_tuning(const pt_renderer* r, pt_tuning* t);
+
+/* ---- measurement ---------------------------------------------------------------------------- */
+
+/* The CUDA stream (a cudaStream_t) on which every device operation of this renderer is ordered, so
+ * that callers can time it with their own events. */
+void* pt_renderer_stream(pt_renderer* r);
+
+enum { PT_PROFILE_KERNEL_TIMES = 1, PT_PROFILE_TRAVERSAL_COUNTS = 2 };
+typedef struct pt_kernel_time { uint64_t launches; double ms; } pt_kernel_time;
+typedef struct pt_profile {
+    pt_kernel_time setup, generate, trace, shade, shadow, accumulate;
+    uint64_t kernel_launches;                       /* every kernel this renderer launched */
+    uint64_t closest_rays, shadow_rays;             /* rays traced (camera + extension, shadow) */
+    uint64_t closest_node_visits, closest_tri_tests;/* with PT_PROFILE_TRAVERSAL_COUNTS */
+    uint64_t shadow_node_visits, shadow_tri_tests;
+} pt_profile;
+/* flags: PT_PROFILE_KERNEL_TIMES records CUDA events between the kernels of every bounce iteration
+ * (inside the captured graphs) and sums each kernel's device time; PT_PROFILE_TRAVERSAL_COUNTS
+ * counts node visits and triangle tests (slower kernels: for a separate, untimed render). */
+int32_t pt_set_profiling(pt_renderer* r, int32_t flags);
+/* Totals since the last pt_set_profiling call. */
+int32_t pt_get_profile(const pt_renderer* r, pt_profile* out);
+
+/* ---- parity probes (the integrator's discrete decisions, for bit-exact checks) -------------- */
+
+/* Primary closest hits of pixel centres + the first random jitter of sample `frame`, exactly the
+ * camera rays of render_sample (pixel.h:18-24): per pixel (t, tri, u, v) into hits4 (4 * w * h floats;
+ * tri is stored as a float bit pattern of the int32, -1 on a miss). */
+int32_t pt_trace_primary(pt_renderer* r, const pt_camera* camera, int32_t width, int32_t height, uint32_t frame,
+                         uint32_t seed, float* hits4);
+/* The light pick of next event estimation at the first vertex of every pixel's sample `frame`
+ * (integrator.h:206-209 with lights.h:139-202): per pixel 4 int32 = group (0 emissive, 1 punctual,
+ * 2 environment, -1 none), index (emissive entry, punctual light, or env row*width+col), alias bin,
+ * 1 if NEE ran at that vertex. */
+int32_t pt_light_picks_primary(pt_renderer* r, const pt_camera* camera, const pt_render_settings* settings,
+                               uint32_t frame, int32_t* picks4);
+/* BVH node visits of the primary ray through each pixel centre (heatmap_kernel,
+ * gpu_renderer.cu:98-106), w * h floats. */
+int32_t pt_heatmap(pt_renderer* r, const pt_camera* camera, int32_t width, int32_t height, float* visits);
+
+/* ---- batched views (one persistent launch over many views) --------------------------------- */
+typedef struct pt_view {
+    pt_camera camera;
+    int32_t width, height, spp;
+    uint32_t seed;
+    pt_path_options path;
+} pt_view;
+/* Renders every view into its own accumulation in one wavefront: work items of all views share
+ * the path pool, bounce iterations run as captured CUDA graphs. Results: pt_download_view. */
+int32_t pt_render_views(pt_renderer* r, const pt_view* views, int32_t n_views);
+int32_t pt_download_view(pt_renderer* r, int32_t view, float* rgb, size_t n);
+
+/* ---- SVGF on caller G-buffers (svgf.h:24-42) --------------------------------------------------
+ * A denoiser session with its own history. Inputs are device pointers to width*height float4:
+ * color, albedo, normal_depth, position (w = material id, -1 miss), emission — the layout of
+ * photon::SvgfInput. output receives the denoised radiance (float4, w = 1). */
+typedef struct pt_svgf pt_svgf;
+int32_t pt_svgf_create(int32_t device, int32_t width, int32_t height, pt_svgf** out);
+void pt_svgf_destroy(pt_svgf* s);
+int32_t pt_svgf_reset(pt_svgf* s);
+int32_t pt_svgf_run(pt_svgf* s, const float* color, const float* albedo, const float* normal_depth,
+                    const float* position, const float* emission, const pt_camera* previous,
+                    const pt_svgf_settings* settings, float* output);
+/* The variance estimate of the last run (Svgf::variance_buffer, svgf.h:44): a device pointer. */
+const float* pt_svgf_variance(const pt_svgf* s);
+const char* pt_svgf_last_error(const pt_svgf* s);
+
+/* ---- request server (continuous batching over resident scenes) ------------------------------ */
+typedef struct pt_server pt_server;
+typedef struct pt_server_config {
+    int32_t device;
+    uint64_t budget_bytes;     /* device memory for scenes + requests + path pool */
+    int32_t path_capacity;     /* shared path pool (0: tuned) */
+    int32_t max_active;        /* requests on the device at once (0: unbounded, budget only) */
+    double device_wait_seconds;/* bound of every device-side wait (0: 2 s) */
+} pt_server_config;
+typedef struct pt_request {
+    int32_t scene_id;
+    pt_camera camera;
+    int32_t width, height, spp;
+    uint32_t seed;
+    pt_path_options path;
+} pt_request;
+enum { PT_REQ_QUEUED = 0, PT_REQ_RUNNING = 1, PT_REQ_DONE = 2, PT_REQ_CANCELLED = 3, PT_REQ_FAILED = 4 };
+typedef struct pt_request_stats {
+    double submit_s, admit_s, done_s;  /* server clock, seconds */
+    uint64_t samples;
+    int32_t state;
+} pt_request_stats;
+typedef struct pt_server_stats {
+    uint64_t submitted, completed, cancelled, rejected;
+    uint64_t samples_done;
+    uint64_t bounce_iterations;
+    uint64_t device_bytes_in_use, budget_bytes;
+    int32_t active, queued, scenes;
+    double busy_seconds;
+} pt_server_stats;
+int32_t pt_server_create(const pt_server_config* cfg, pt_server** out);
+void pt_server_destroy(pt_server* s);
+const char* pt_server_last_error(const pt_server* s);
+/* Makes a scene resident (copied) and returns its id. PT_ERR_BUDGET when it does not fit. */
+int32_t pt_server_add_scene(pt_server* s, const pt_scene_desc* scene, int32_t* scene_id);
+/* Non-blocking. Fails with PT_ERR_BUDGET when the request alone can never fit the budget. */
+int32_t pt_server_submit(pt_server* s, const pt_request* req, uint64_t* request_id);
+int32_t pt_server_poll(pt_server* s, uint64_t request_id, int32_t* state);
+/* Waits up to timeout_s for the request to finish (PT_ERR_TIMEOUT otherwise). */
+int32_t pt_server_wait(pt_server* s, uint64_t request_id, double timeout_s);
+/* Copies a finished request's average radiance (3 floats/pixel) and releases it. */
+int32_t pt_server_fetch(pt_server* s, uint64_t request_id, float* rgb, size_t n, pt_request_stats* st);
+int32_t pt_server_cancel(pt_server* s, uint64_t request_id);
+int32_t pt_server_get_stats(pt_server* s, pt_server_stats* out);
+/* Test hook (host-side fault injection): the next `count` device allocations of request buffers
+ * fail, so the affected requests end in PT_REQ_FAILED without touching the GPU. */
+int32_t pt_server_debug_fail_allocations(pt_server* s, int32_t count);
+
+/* ---- scene construction (host) ----------------------------------------------------------------
+ * Photon builds scenes on the host (Scene::build, scene.cpp:212-255). The library carries its own
+ * builder so that servers and benchmarks can admit procedural scenes without Photon's host code:
+ * pt_scene_build turns raw meshes into the pt_scene_desc arrays (binned SAH BVH with 2-child 64-byte
+ * nodes, alias table, environment CDFs). */
+typedef struct pt_texture_desc {
+    int32_t width, height;
+    const uint32_t* texels;  /* RGBA8, row 0 at the top */
+    int32_t repeat, srgb;
+} pt_texture_desc;
+typedef struct pt_raw_scene {
+    const pt_vec3* positions; int32_t num_positions;
+    const pt_vec3* normals;   /* num_positions or NULL */
+    const pt_vec2* uvs;       /* num_positions or NULL */
+    const pt_vec4* tangents;  /* num_positions or NULL */
+    const int32_t* indices; int32_t num_indices;
+    const int32_t* tri_material;   /* num_indices / 3 */
+    const pt_material* materials; int32_t num_materials;
+    const pt_texture_desc* textures; int32_t num_textures;
+    const pt_punctual_light* punctual; int32_t num_punctual;
+    const pt_vec3* env_texels; int32_t env_width, env_height;
+    pt_vec3 env_color; float env_intensity, env_rotation;
+} pt_raw_scene;
+typedef struct pt_built_scene pt_built_scene;
+typedef struct pt_bvh_build_options { int32_t bins, max_leaf_size; float traversal_cost; int32_t threads; } pt_bvh_build_options;
+int32_t pt_scene_build(const pt_raw_scene* raw, const pt_bvh_build_options* opt, pt_built_scene** out);
+/* The built arrays; valid until pt_scene_free. */
+const pt_scene_desc* pt_scene_desc_of(const pt_built_scene* b);
+void pt_scene_free(pt_built_scene* b);
+
+/* Procedural scenes of the benchmark configurations. kind:
+ *   PT_GEN_BOX      the closed box: 5 walls, 2 rotated boxes, a ceiling emitter (36 triangles);
+ *   PT_GEN_TERRAIN  the height-field scene: value-noise terrain, instanced spheres and cylinders
+ *                   (10% mirrored), 64 materials (25% alpha-masked checker), 64 emissive triangles,
+ *                   4 point/spot lights, a 1024x512 HDR sky with 3 lobes. triangles = total count
+ *                   (262144 for the 262K scene; larger counts scale the tessellation). */
+enum { PT_GEN_BOX = 0, PT_GEN_TERRAIN = 1 };
+typedef struct pt_generated pt_generated;
+int32_t pt_generate_scene(int32_t kind, int64_t triangles, uint64_t seed, pt_generated** out);
+const pt_raw_scene* pt_generated_raw(const pt_generated* g);
+/* The scene's default camera for an aspect ratio. */
+int32_t pt_generated_camera(const pt_generated* g, float aspect, pt_camera* out);
+void pt_generated_free(pt_generated* g);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHOTON_WAVEFRONT_H */

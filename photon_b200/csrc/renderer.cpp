@@ -1,0 +1,658 @@
+// The wavefront engine (path pool, device counters, CUDA-graph iterations) and the drop-in renderer
+// that replaces photon::GpuRenderer (src/render/gpu_renderer.cu:177-454 of Photon).
+#include "renderer.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+
+#include "svgf.h"
+
+namespace ptw {
+
+// ---- WavefrontEngine ------------------------------------------------------------------------------------
+
+WavefrontEngine::WavefrontEngine(int device, cudaStream_t stream) : device_(device), stream_(stream) {
+    PTW_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_ctr_), sizeof(Counters)));
+    std::memset(h_ctr_, 0, sizeof(Counters));
+    PTW_CUDA(cudaEventCreateWithFlags(&ev_, cudaEventDisableTiming));
+    ctr_.allocate(1);
+}
+
+WavefrontEngine::~WavefrontEngine() {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    for (cudaEvent_t e : prof_ev_) cudaEventDestroy(e);
+    if (ev_) cudaEventDestroy(ev_);
+    if (h_ctr_) cudaFreeHost(h_ctr_);
+}
+
+void WavefrontEngine::set_tuning(const Tuning& t) {
+    bool reshape = t.trace_block != tuning_.trace_block || t.shade_block != tuning_.shade_block;
+    bool realloc = t.path_capacity != tuning_.path_capacity;
+    tuning_ = t;
+    if (reshape) shape_ok_ = false;
+    if (realloc) {
+        for (auto& b : bufs_) b.release();
+        for (auto& b : ids_) b.release();
+        pb_ = PathBuffers{};
+    }
+    if (graph_) {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+}
+
+void WavefrontEngine::set_profiling(int flags) {
+    profile_flags_ = flags;
+    for (double& m : kernel_ms) m = 0;
+    kernel_launches = iteration_launches = 0;
+    if (graph_) {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+    int need = 6 * std::max(1, tuning_.graph_bounces);
+    while (int(prof_ev_.size()) < need) {
+        cudaEvent_t e;
+        PTW_CUDA(cudaEventCreate(&e));
+        prof_ev_.push_back(e);
+    }
+}
+
+void WavefrontEngine::collect_kernel_times(int iterations) {
+    for (int k = 0; k < iterations; k++)
+        for (int j = 0; j < 5; j++) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, prof_ev_[size_t(6 * k + j)], prof_ev_[size_t(6 * k + j + 1)]) == cudaSuccess) kernel_ms[j] += ms;
+        }
+}
+
+uint64_t WavefrontEngine::bytes_per_path() const { return 12 * 16 + 2 * 16; }
+
+void WavefrontEngine::reserve_paths(uint64_t needed) {
+    uint64_t want = std::min<uint64_t>(uint64_t(tuning_.path_capacity), (needed + 1023) / 1024 * 1024);
+    if (want < 1024) want = 1024;
+    if (pb_.capacity >= want) return;
+    for (auto& b : bufs_) b.allocate(want);
+    for (auto& b : ids_) b.allocate(want);
+    for (int k = 0; k < 2; k++) {
+        pb_.o[k] = bufs_[0 + k].ptr;
+        pb_.d[k] = bufs_[2 + k].ptr;
+        pb_.beta[k] = bufs_[4 + k].ptr;
+        pb_.lr[k] = bufs_[6 + k].ptr;
+        pb_.id[k] = ids_[k].ptr;
+    }
+    pb_.hit = bufs_[8].ptr;
+    pb_.sh0 = bufs_[9].ptr;
+    pb_.sh1 = bufs_[10].ptr;
+    pb_.sh2 = bufs_[11].ptr;
+    pb_.capacity = uint32_t(want);
+    if (graph_) {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+}
+
+size_t WavefrontEngine::device_bytes() const {
+    size_t b = ctr_.bytes();
+    for (const auto& x : bufs_) b += x.bytes();
+    for (const auto& x : ids_) b += x.bytes();
+    return b;
+}
+
+void WavefrontEngine::ensure_shape() {
+    if (shape_ok_) return;
+    PTW_CUDA(wf_launch_shape(device_, tuning_.trace_block, tuning_.shade_block, &shape_));
+    shape_ok_ = true;
+}
+
+WfParams WavefrontEngine::params(const DevScene* scenes, int single, const DevView* views, int n, bool count) const {
+    WfParams p{};
+    p.scenes = scenes;
+    p.views = views;
+    p.num_views = n;
+    p.single_scene = single;
+    p.pb = pb_;
+    p.ctr = ctr_.ptr;
+    p.count_work = count ? 1 : 0;
+    return p;
+}
+
+void WavefrontEngine::capture(const WfParams& p) {
+    if (graph_) {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+    int iters = std::max(1, tuning_.graph_bounces);
+    cudaGraph_t g = nullptr;
+    bool timed = (profile_flags_ & PT_PROFILE_KERNEL_TIMES) && int(prof_ev_.size()) >= 6 * iters;
+    PTW_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < iters; k++) wf_iteration(p, shape_, stream_, timed ? &prof_ev_[size_t(6 * k)] : nullptr);
+    cudaMemcpyAsync(h_ctr_, ctr_.ptr, sizeof(Counters), cudaMemcpyDeviceToHost, stream_);
+    cudaError_t e = cudaStreamEndCapture(stream_, &g);
+    if (e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        throw Error{PT_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(e)};
+    }
+    e = cudaGraphInstantiate(&graph_, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        graph_ = nullptr;
+        throw Error{PT_ERR_CUDA, std::string("graph instantiation failed: ") + cudaGetErrorString(e)};
+    }
+    graph_params_ = p;
+    graph_iters_ = iters;
+}
+
+void WavefrontEngine::run(const DevScene* scenes, int single_scene, const DevView* views, int n_views, uint64_t total_work,
+                          bool count_work) {
+    if (total_work == 0) return;
+    reserve_paths(total_work);
+    ensure_shape();
+    std::memset(h_ctr_, 0, sizeof(Counters));
+    h_ctr_->parity = 1;
+    h_ctr_->work_total = total_work;
+    PTW_CUDA(cudaMemcpyAsync(ctr_.ptr, h_ctr_, sizeof(Counters), cudaMemcpyHostToDevice, stream_));
+    WfParams p = params(scenes, single_scene, views, n_views, count_work || (profile_flags_ & PT_PROFILE_TRAVERSAL_COUNTS));
+    bool use_graph = tuning_.graph_bounces > 0;
+    bool timed = (profile_flags_ & PT_PROFILE_KERNEL_TIMES) != 0;
+    if (use_graph && (!graph_ || std::memcmp(&graph_params_, &p, sizeof(p)) != 0 || graph_iters_ != tuning_.graph_bounces)) capture(p);
+    const uint64_t max_launches = 1u << 22;
+    for (uint64_t launch = 0;; launch++) {
+        int iters = use_graph ? graph_iters_ : 1;
+        if (use_graph) {
+            PTW_CUDA(cudaGraphLaunch(graph_, stream_));
+        } else {
+            PTW_CUDA(wf_iteration(p, shape_, stream_, timed ? prof_ev_.data() : nullptr));
+            PTW_CUDA(cudaMemcpyAsync(h_ctr_, ctr_.ptr, sizeof(Counters), cudaMemcpyDeviceToHost, stream_));
+        }
+        PTW_CUDA(cudaEventRecord(ev_, stream_));
+        PTW_CUDA(cudaEventSynchronize(ev_));
+        kernel_launches += uint64_t(iters) * kKernelsPerIteration;
+        iteration_launches += uint64_t(iters);
+        if (timed) collect_kernel_times(iters);
+        const Counters& h = *h_ctr_;
+        if (h.count[h.parity ^ 1u] == 0 && h.work_next >= h.work_total) break;
+        if (launch > max_launches) throw Error{PT_ERR_TIMEOUT, "wavefront did not drain"};
+    }
+    last_ = *h_ctr_;
+}
+
+void WavefrontEngine::begin(const DevScene* scenes, const DevView* views, int n_views) {
+    ensure_shape();
+    std::memset(h_ctr_, 0, sizeof(Counters));
+    h_ctr_->parity = 1;
+    PTW_CUDA(cudaMemcpyAsync(ctr_.ptr, h_ctr_, sizeof(Counters), cudaMemcpyHostToDevice, stream_));
+    cont_params_ = params(scenes, -1, views, n_views, false);
+}
+
+void WavefrontEngine::set_views(const DevView* views, int n_views) {
+    cont_params_.views = views;
+    cont_params_.num_views = n_views;
+    cont_params_.pb = pb_;
+}
+
+void WavefrontEngine::append_work(uint64_t new_total) {
+    static_assert(sizeof(unsigned long long) == 8, "counter width");
+    // A stream-ordered write of work_total between iterations (the kernels read it in setup).
+    // The value is staged in a pinned slot so that the copy reads it at execution time.
+    h_ctr_->work_total = new_total;
+    PTW_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(ctr_.ptr) + offsetof(Counters, work_total), &h_ctr_->work_total,
+                             sizeof(unsigned long long), cudaMemcpyHostToDevice, stream_));
+    PTW_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void WavefrontEngine::iterate(int iterations) {
+    for (int k = 0; k < iterations; k++) PTW_CUDA(wf_iteration(cont_params_, shape_, stream_));
+    kernel_launches += uint64_t(iterations) * kKernelsPerIteration;
+    iteration_launches += uint64_t(iterations);
+    PTW_CUDA(cudaMemcpyAsync(h_ctr_, ctr_.ptr, sizeof(Counters), cudaMemcpyDeviceToHost, stream_));
+}
+
+void WavefrontEngine::sync() {
+    PTW_CUDA(cudaEventRecord(ev_, stream_));
+    PTW_CUDA(cudaEventSynchronize(ev_));
+}
+
+// ---- Renderer ----------------------------------------------------------------------------------------------
+
+Renderer::Renderer(int device) : device_(device) {
+    PTW_CUDA(cudaSetDevice(device));
+    PTW_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    engine_ = std::make_unique<WavefrontEngine>(device, stream_);
+    PTW_CUDA(cudaEventCreate(&ev0_));
+    PTW_CUDA(cudaEventCreate(&ev1_));
+    PTW_CUDA(cudaEventCreate(&acc_ev_[0]));
+    PTW_CUDA(cudaEventCreate(&acc_ev_[1]));
+    d_views_.allocate(1);
+}
+
+Renderer::~Renderer() {
+    cudaSetDevice(device_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    svgf_.reset();
+    engine_.reset();
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    for (cudaEvent_t e : acc_ev_)
+        if (e) cudaEventDestroy(e);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Renderer::upload(const pt_scene_desc& d, bool lights_only) {
+    PTW_CUDA(cudaSetDevice(device_));
+    scene_.upload(d, stream_, lights_only);
+    if (width_ > 0) reset();
+    else {
+        samples_ = 0;
+        frame_ = 0;
+        denoised_ = false;
+    }
+}
+
+void Renderer::resize(int w, int h) {
+    if (w < 0 || h < 0) throw Error{PT_ERR_INVALID, "negative image size"};
+    if (w == width_ && h == height_ && accum_.count) return;
+    PTW_CUDA(cudaSetDevice(device_));
+    width_ = w;
+    height_ = h;
+    size_t n = size_t(w) * size_t(h);
+    for (DeviceBuffer<float4>* b : {&accum_, &albedo_, &normal_depth_, &position_, &emission_, &color_, &denoised_buf_}) {
+        b->allocate(n);
+        b->zero(stream_);
+    }
+    heat_.allocate(n);
+    display_.allocate(n);
+    display_.zero(stream_);
+    if (!svgf_) svgf_ = std::make_unique<SvgfDenoiser>(device_, stream_);
+    svgf_->resize(w, h);
+    PTW_CUDA(cudaStreamSynchronize(stream_));
+    reset();
+}
+
+void Renderer::reset() {
+    samples_ = 0;
+    frame_ = 0;
+    denoised_ = false;
+    heat_valid_ = false;
+    accum_.zero(stream_);
+    if (svgf_) svgf_->reset();
+    PTW_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Renderer::fill_view(DevView& v, const pt_camera& cam, int w, int h, int spp, uint32_t seed, const pt_path_options& po,
+                         uint32_t frame0) const {
+    // The path depth lives in 16 bits of the path state.
+    if (po.max_depth < 0 || po.max_depth > 65535) throw Error{PT_ERR_INVALID, "max_depth must be in [0, 65535]"};
+    if (w < 0 || h < 0 || spp < 0) throw Error{PT_ERR_INVALID, "negative image size or spp"};
+    std::memset(&v, 0, sizeof(v));
+    std::memcpy(v.cam, &cam, sizeof(v.cam));
+    v.width = w;
+    v.height = h;
+    v.spp = spp;
+    v.scene = 0;
+    v.seed = seed;
+    v.frame0 = frame0;
+    v.max_depth = po.max_depth;
+    v.rr_depth = po.rr_depth;
+    v.nee = po.nee;
+    v.clamp = po.clamp;
+}
+
+// Renders a set of views (each with its own spp and first sample index) in passes that fit the
+// radiance buffer: work units are (view, sample range) packed in order; each unit's samples are
+// summed into its view's accumulation in sample order after its pass.
+void Renderer::render_pass_set(std::vector<DevView>& views, int /*spp_total*/, std::vector<int>& spp_each, std::vector<uint32_t>& frame0) {
+    struct Unit {
+        int view, s0, s1;
+    };
+    std::vector<std::vector<Unit>> passes(1);
+    uint64_t used = 0;
+    for (size_t vi = 0; vi < views.size(); vi++) {
+        uint64_t npix = uint64_t(views[vi].width) * uint64_t(views[vi].height);
+        if (npix == 0 || spp_each[vi] <= 0) continue;
+        int s = 0;
+        while (s < spp_each[vi]) {
+            uint64_t room = sample_cap_ > used ? sample_cap_ - used : 0;
+            int take = int(std::min<uint64_t>(uint64_t(spp_each[vi] - s), room / npix));
+            if (take <= 0) {
+                if (used == 0) take = 1;  // a single sample row larger than the cap: one pass of its own
+                else {
+                    passes.emplace_back();
+                    used = 0;
+                    continue;
+                }
+            }
+            passes.back().push_back({int(vi), s, s + take});
+            used += uint64_t(take) * npix;
+            s += take;
+        }
+    }
+    for (const auto& pass : passes) {
+        if (pass.empty()) continue;
+        std::vector<DevView> table;
+        uint64_t work = 0;
+        for (const Unit& u : pass) {
+            DevView v = views[size_t(u.view)];
+            uint64_t npix = uint64_t(v.width) * uint64_t(v.height);
+            v.spp = u.s1 - u.s0;
+            v.frame0 = frame0[size_t(u.view)] + uint32_t(u.s0);
+            v.gbuffer = (u.s0 == 0) ? v.gbuffer : 0;
+            v.realtime = (u.s0 == 0) ? v.realtime : 0;
+            v.work_begin = work;
+            v.work_count = npix * uint64_t(v.spp);
+            table.push_back(v);
+            work += v.work_count;
+        }
+        sample_out_.reserve(work);
+        uint64_t off = 0;
+        for (DevView& v : table) {
+            v.sample_out = sample_out_.ptr + off;
+            off += v.work_count;
+        }
+        if (d_views_.count < table.size()) d_views_.allocate(table.size());
+        PTW_CUDA(cudaMemcpyAsync(d_views_.ptr, table.data(), table.size() * sizeof(DevView), cudaMemcpyHostToDevice, stream_));
+        engine_->run(scene_.device_view(), 0, d_views_.ptr, int(table.size()), work);
+        last_ctr_ = engine_->last();
+        profile_.closest_rays += last_ctr_.rays;
+        profile_.shadow_rays += last_ctr_.shadow_rays;
+        profile_.closest_node_visits += last_ctr_.node_visits;
+        profile_.closest_tri_tests += last_ctr_.tri_tests;
+        profile_.shadow_node_visits += last_ctr_.shadow_node_visits;
+        profile_.shadow_tri_tests += last_ctr_.shadow_tri_tests;
+        bool timed = engine_->profiling() & PT_PROFILE_KERNEL_TIMES;
+        if (timed) PTW_CUDA(cudaEventRecord(acc_ev_[0], stream_));
+        for (size_t k = 0; k < table.size(); k++) {
+            const Unit& u = pass[k];
+            int first = u.s0 == 0, last = u.s1 == spp_each[size_t(u.view)];
+            PTW_CUDA(wf_accumulate(d_views_.ptr + k, table[k], first, last, stream_));
+        }
+        profile_.accumulate.launches += table.size();
+        profile_.kernel_launches += table.size();
+        if (timed) PTW_CUDA(cudaEventRecord(acc_ev_[1], stream_));
+        PTW_CUDA(cudaStreamSynchronize(stream_));
+        if (timed) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, acc_ev_[0], acc_ev_[1]);
+            profile_.accumulate.ms += ms;
+        }
+    }
+}
+
+void Renderer::render(const pt_camera& cam, const pt_render_settings& rs, int spp) {
+    if (!scene_.ready()) throw Error{PT_ERR_NO_SCENE, "render before upload"};
+    if (width_ == 0 || height_ == 0 || spp <= 0) return;
+    PTW_CUDA(cudaSetDevice(device_));
+    if (denoised_) reset();
+    uint64_t npix = uint64_t(width_) * uint64_t(height_);
+    DevView v;
+    fill_view(v, cam, width_, height_, spp, rs.seed, rs.path, uint32_t(samples_));
+    v.gbuffer = 1;
+    v.accum = accum_.ptr;
+    v.g_albedo = albedo_.ptr;
+    v.g_normal_depth = normal_depth_.ptr;
+    if (uint64_t(spp) * npix > sample_cap_) {
+        acc_pass_.reserve(npix);
+        v.acc_pass = acc_pass_.ptr;
+    }
+    std::vector<DevView> views{v};
+    std::vector<int> spps{spp};
+    std::vector<uint32_t> f0{uint32_t(samples_)};
+    PTW_CUDA(cudaEventRecord(ev0_, stream_));
+    render_pass_set(views, spp, spps, f0);
+    PTW_CUDA(cudaEventRecord(ev1_, stream_));
+    PTW_CUDA(cudaEventSynchronize(ev1_));
+    cudaEventElapsedTime(&last_ms_, ev0_, ev1_);
+    samples_ += spp;
+    last_camera_ = cam;
+    heat_valid_ = false;
+}
+
+void Renderer::render_denoised(const pt_camera& cam, const pt_camera& prev, const pt_render_settings& rs, const pt_svgf_settings& sv) {
+    if (!scene_.ready()) throw Error{PT_ERR_NO_SCENE, "render before upload"};
+    if (width_ == 0 || height_ == 0) return;
+    PTW_CUDA(cudaSetDevice(device_));
+    if (!denoised_) {
+        samples_ = 0;
+        svgf_->reset();
+    }
+    denoised_ = true;
+    DevView v;
+    fill_view(v, cam, width_, height_, 1, rs.seed, rs.path, frame_);
+    v.gbuffer = 1;
+    v.realtime = 1;
+    // The real-time sample is not accumulated: its radiance goes to `color` only.
+    acc_pass_.reserve(size_t(width_) * size_t(height_));
+    v.accum = acc_pass_.ptr;
+    v.g_albedo = albedo_.ptr;
+    v.g_normal_depth = normal_depth_.ptr;
+    v.g_position = position_.ptr;
+    v.g_emission = emission_.ptr;
+    v.g_color = color_.ptr;
+    std::vector<DevView> views{v};
+    std::vector<int> spps{1};
+    std::vector<uint32_t> f0{frame_};
+    PTW_CUDA(cudaEventRecord(ev0_, stream_));
+    render_pass_set(views, 1, spps, f0);
+    svgf_->run(reinterpret_cast<const float*>(color_.ptr), reinterpret_cast<const float*>(albedo_.ptr),
+               reinterpret_cast<const float*>(normal_depth_.ptr), reinterpret_cast<const float*>(position_.ptr),
+               reinterpret_cast<const float*>(emission_.ptr), prev, sv, reinterpret_cast<float*>(denoised_buf_.ptr));
+    PTW_CUDA(cudaEventRecord(ev1_, stream_));
+    PTW_CUDA(cudaEventSynchronize(ev1_));
+    cudaEventElapsedTime(&last_ms_, ev0_, ev1_);
+    frame_++;
+    samples_ = 1;
+    last_camera_ = cam;
+    heat_valid_ = false;
+}
+
+void Renderer::display(const pt_render_settings& rs, int mode, uint32_t* target) {
+    if (width_ == 0) return;
+    PTW_CUDA(cudaSetDevice(device_));
+    if (mode == PT_DISPLAY_HEATMAP && !heat_valid_ && scene_.ready()) {
+        PTW_CUDA(wf_heatmap(scene_.device_view(), reinterpret_cast<const float*>(&last_camera_), width_, height_, heat_.ptr, stream_));
+        heat_valid_ = true;
+    }
+    DisplayParams p;
+    p.w = width_;
+    p.h = height_;
+    p.mode = mode;
+    p.exposure = rs.exposure;
+    p.tonemap = rs.tonemap;
+    p.samples = float(samples_);
+    p.inv_samples = samples_ > 0 ? 1.0f / float(samples_) : 0.0f;
+    p.max_depth = scene_.extent();
+    p.heat_scale = 1.0f / 160.0f;
+    p.denoised = denoised_ ? 1 : 0;
+    const float4* variance = svgf_ ? reinterpret_cast<const float4*>(svgf_->variance()) : nullptr;
+    PTW_CUDA(wf_display(p, accum_.ptr, denoised_buf_.ptr, albedo_.ptr, normal_depth_.ptr, variance, heat_.ptr,
+                        target ? target : display_.ptr, stream_));
+    PTW_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Renderer::download_image(float* rgb, size_t n) {
+    size_t npix = size_t(width_) * size_t(height_);
+    if (n < 3 * npix) throw Error{PT_ERR_INVALID, "download_image: buffer too small"};
+    if (npix == 0) return;
+    std::vector<float4> raw(npix);
+    PTW_CUDA(cudaMemcpyAsync(raw.data(), denoised_ ? denoised_buf_.ptr : accum_.ptr, npix * sizeof(float4), cudaMemcpyDeviceToHost, stream_));
+    PTW_CUDA(cudaStreamSynchronize(stream_));
+    if (denoised_) {
+        for (size_t i = 0; i < npix; i++) {
+            rgb[3 * i] = raw[i].x;
+            rgb[3 * i + 1] = raw[i].y;
+            rgb[3 * i + 2] = raw[i].z;
+        }
+    } else {
+        // vec3 * (1 / samples), as GpuRenderer::download_image and CpuRenderer::image.
+        float inv = samples_ > 0 ? 1.0f / float(samples_) : 0.0f;
+        for (size_t i = 0; i < npix; i++) {
+            rgb[3 * i] = raw[i].x * inv;
+            rgb[3 * i + 1] = raw[i].y * inv;
+            rgb[3 * i + 2] = raw[i].z * inv;
+        }
+    }
+}
+
+void Renderer::download_display(uint32_t* out, size_t n) {
+    size_t npix = size_t(width_) * size_t(height_);
+    if (n < npix) throw Error{PT_ERR_INVALID, "download_display: buffer too small"};
+    if (npix) {
+        PTW_CUDA(cudaMemcpyAsync(out, display_.ptr, npix * 4, cudaMemcpyDeviceToHost, stream_));
+        PTW_CUDA(cudaStreamSynchronize(stream_));
+    }
+}
+
+void Renderer::download_gbuffer(float* albedo4, float* nd4, size_t n) {
+    size_t npix = size_t(width_) * size_t(height_);
+    if (n < npix) throw Error{PT_ERR_INVALID, "download_gbuffer: buffer too small"};
+    if (albedo4) PTW_CUDA(cudaMemcpyAsync(albedo4, albedo_.ptr, npix * 16, cudaMemcpyDeviceToHost, stream_));
+    if (nd4) PTW_CUDA(cudaMemcpyAsync(nd4, normal_depth_.ptr, npix * 16, cudaMemcpyDeviceToHost, stream_));
+    PTW_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Renderer::stats(pt_stats* out) const {
+    std::memset(out, 0, sizeof(*out));
+    out->width = width_;
+    out->height = height_;
+    out->samples = samples_;
+    out->last_frame_ms = last_ms_;
+    out->paths = last_ctr_.work_total;
+    out->rays = last_ctr_.rays + last_ctr_.shadow_rays;
+    out->shadow_rays = last_ctr_.shadow_rays;
+    out->bounce_iterations = last_ctr_.iterations;
+    out->queue_overflows = last_ctr_.overflow;
+    size_t b = scene_.device_bytes() + engine_->device_bytes() + sample_out_.bytes() + heat_.bytes() + display_.bytes();
+    for (const DeviceBuffer<float4>* x : {&accum_, &acc_pass_, &albedo_, &normal_depth_, &position_, &emission_, &color_, &denoised_buf_}) b += x->bytes();
+    out->device_bytes = b;
+}
+
+void Renderer::set_profiling(int flags) {
+    engine_->set_profiling(flags);
+    profile_ = pt_profile{};
+}
+
+void Renderer::get_profile(pt_profile* out) const {
+    *out = profile_;
+    const WavefrontEngine& e = *engine_;
+    pt_kernel_time* k[5] = {&out->setup, &out->generate, &out->trace, &out->shade, &out->shadow};
+    for (int j = 0; j < 5; j++) {
+        k[j]->launches = e.iteration_launches;
+        k[j]->ms = e.kernel_ms[j];
+    }
+    out->kernel_launches = profile_.kernel_launches + e.kernel_launches;
+}
+
+void Renderer::set_tuning(const pt_tuning& t) {
+    Tuning cur = engine_->tuning();
+    if (t.path_capacity > 0) cur.path_capacity = t.path_capacity;
+    if (t.trace_block > 0) {
+        if (t.trace_block % 32 || t.trace_block > 256) throw Error{PT_ERR_INVALID, "trace_block must be a multiple of 32, at most 256"};
+        cur.trace_block = t.trace_block;
+    }
+    if (t.shade_block > 0) {
+        if (t.shade_block % 32 || t.shade_block > 256) throw Error{PT_ERR_INVALID, "shade_block must be a multiple of 32, at most 256"};
+        cur.shade_block = t.shade_block;
+    }
+    if (t.sort_by_material >= 0) cur.sort_by_material = t.sort_by_material;
+    if (t.graph_bounces >= 0) cur.graph_bounces = t.graph_bounces;
+    engine_->set_tuning(cur);
+}
+
+void Renderer::get_tuning(pt_tuning* t) const {
+    const Tuning& c = engine_->tuning();
+    t->path_capacity = c.path_capacity;
+    t->trace_block = c.trace_block;
+    t->shade_block = c.shade_block;
+    t->sort_by_material = c.sort_by_material;
+    t->graph_bounces = c.graph_bounces;
+}
+
+void Renderer::trace_primary(const pt_camera& cam, int w, int h, uint32_t frame, uint32_t seed, float* hits4) {
+    if (!scene_.ready()) throw Error{PT_ERR_NO_SCENE, "trace before upload"};
+    if (w <= 0 || h <= 0) return;
+    PTW_CUDA(cudaSetDevice(device_));
+    DeviceBuffer<float4> out;
+    out.allocate(size_t(w) * size_t(h));
+    PTW_CUDA(wf_trace_primary(scene_.device_view(), reinterpret_cast<const float*>(&cam), w, h, frame, seed, out.ptr, stream_));
+    PTW_CUDA(cudaMemcpyAsync(hits4, out.ptr, out.bytes(), cudaMemcpyDeviceToHost, stream_));
+    PTW_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Renderer::light_picks(const pt_camera& cam, const pt_render_settings& rs, uint32_t frame, int32_t* picks4) {
+    if (!scene_.ready()) throw Error{PT_ERR_NO_SCENE, "probe before upload"};
+    if (rs.width <= 0 || rs.height <= 0) return;
+    PTW_CUDA(cudaSetDevice(device_));
+    DevView v;
+    fill_view(v, cam, rs.width, rs.height, 1, rs.seed, rs.path, frame);
+    DeviceBuffer<DevView> dv;
+    dv.upload(&v, 1, stream_);
+    DeviceBuffer<int4> out;
+    out.allocate(size_t(rs.width) * size_t(rs.height));
+    PTW_CUDA(wf_light_picks(scene_.device_view(), dv.ptr, out.ptr, rs.width, rs.height, stream_));
+    PTW_CUDA(cudaMemcpyAsync(picks4, out.ptr, out.bytes(), cudaMemcpyDeviceToHost, stream_));
+    PTW_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Renderer::heatmap(const pt_camera& cam, int w, int h, float* out) {
+    if (!scene_.ready()) throw Error{PT_ERR_NO_SCENE, "probe before upload"};
+    if (w <= 0 || h <= 0) return;
+    PTW_CUDA(cudaSetDevice(device_));
+    DeviceBuffer<float> buf;
+    buf.allocate(size_t(w) * size_t(h));
+    PTW_CUDA(wf_heatmap(scene_.device_view(), reinterpret_cast<const float*>(&cam), w, h, buf.ptr, stream_));
+    PTW_CUDA(cudaMemcpyAsync(out, buf.ptr, buf.bytes(), cudaMemcpyDeviceToHost, stream_));
+    PTW_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Renderer::render_views(const pt_view* views, int n) {
+    if (!scene_.ready()) throw Error{PT_ERR_NO_SCENE, "render before upload"};
+    if (n < 0) throw Error{PT_ERR_INVALID, "negative view count"};
+    PTW_CUDA(cudaSetDevice(device_));
+    batch_views_.assign(views, views + n);
+    batch_accum_.resize(size_t(n));
+    std::vector<DevView> table(static_cast<size_t>(n));
+    std::vector<int> spps(static_cast<size_t>(n));
+    std::vector<uint32_t> f0(size_t(n), 0);
+    static thread_local std::vector<DeviceBuffer<float4>> pass_bufs;
+    pass_bufs.resize(size_t(n));
+    for (int i = 0; i < n; i++) {
+        const pt_view& pv = views[i];
+        if (pv.width < 0 || pv.height < 0 || pv.spp < 0) throw Error{PT_ERR_INVALID, "bad view size"};
+        size_t npix = size_t(pv.width) * size_t(pv.height);
+        batch_accum_[size_t(i)].allocate(npix);
+        batch_accum_[size_t(i)].zero(stream_);
+        fill_view(table[size_t(i)], pv.camera, pv.width, pv.height, pv.spp, pv.seed, pv.path, 0);
+        table[size_t(i)].accum = batch_accum_[size_t(i)].ptr;
+        if (uint64_t(pv.spp) * npix > sample_cap_) {
+            pass_bufs[size_t(i)].reserve(npix);
+            table[size_t(i)].acc_pass = pass_bufs[size_t(i)].ptr;
+        }
+        spps[size_t(i)] = pv.spp;
+    }
+    PTW_CUDA(cudaEventRecord(ev0_, stream_));
+    render_pass_set(table, 0, spps, f0);
+    PTW_CUDA(cudaEventRecord(ev1_, stream_));
+    PTW_CUDA(cudaEventSynchronize(ev1_));
+    cudaEventElapsedTime(&last_ms_, ev0_, ev1_);
+}
+
+void Renderer::download_view(int v, float* rgb, size_t n) {
+    if (v < 0 || size_t(v) >= batch_views_.size()) throw Error{PT_ERR_NOT_FOUND, "no such view"};
+    const pt_view& pv = batch_views_[size_t(v)];
+    size_t npix = size_t(pv.width) * size_t(pv.height);
+    if (n < 3 * npix) throw Error{PT_ERR_INVALID, "download_view: buffer too small"};
+    std::vector<float4> raw(npix);
+    if (npix) {
+        PTW_CUDA(cudaMemcpyAsync(raw.data(), batch_accum_[size_t(v)].ptr, npix * 16, cudaMemcpyDeviceToHost, stream_));
+        PTW_CUDA(cudaStreamSynchronize(stream_));
+    }
+    float inv = pv.spp > 0 ? 1.0f / float(pv.spp) : 0.0f;
+    for (size_t i = 0; i < npix; i++) {
+        rgb[3 * i] = raw[i].x * inv;
+        rgb[3 * i + 1] = raw[i].y * inv;
+        rgb[3 * i + 2] = raw[i].z * inv;
+    }
+}
+
+}  // namespace ptw

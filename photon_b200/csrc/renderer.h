@@ -1,0 +1,160 @@
+// The wavefront engine and the drop-in renderer built on it (host side).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "device_scene.h"
+#include "wavefront.h"
+
+namespace ptw {
+
+class SvgfDenoiser;
+
+// Tunable launch parameters (the autotuner's knobs).
+struct Tuning {
+    int path_capacity = 1 << 21;   // paths in flight
+    int trace_block = 128;
+    int shade_block = 128;
+    int sort_by_material = 0;
+    int graph_bounces = 4;         // iterations per CUDA graph launch
+};
+
+// Runs wavefront passes over a table of views on one device stream. Owns the path pool, the
+// counters and the captured iteration graph.
+class WavefrontEngine {
+public:
+    WavefrontEngine(int device, cudaStream_t stream);
+    ~WavefrontEngine();
+
+    void set_tuning(const Tuning& t);
+    const Tuning& tuning() const { return tuning_; }
+
+    // Makes sure the pool holds at least min(capacity, needed) paths.
+    void reserve_paths(uint64_t needed);
+
+    // Renders one pass: every work item of `views` (device table of n views, work ranges
+    // contiguous from 0) until all paths finished. scenes: device table; single_scene >= 0 when
+    // all views share that slot. Blocks the host until done (bounded by max_iterations).
+    void run(const DevScene* scenes, int single_scene, const DevView* views, int n_views, uint64_t total_work,
+             bool count_work = false);
+
+    // Continuous mode (the request server): prepare once, then alternate iterate() with host-side
+    // admission of new work (append_work) and completion checks (counters()).
+    void begin(const DevScene* scenes, const DevView* views, int n_views);
+    void set_views(const DevView* views, int n_views);
+    void append_work(uint64_t new_total);   // raises work_total (stream-ordered)
+    void iterate(int iterations);           // launches iterations and copies the counters back
+    const Counters& counters() const { return *h_ctr_; }  // valid after sync()
+    void sync();
+
+    const Counters& last() const { return last_; }
+
+    // Profiling (pt_set_profiling): per-kernel device time recorded by events inside the graphs,
+    // and traversal counters in the kernels.
+    void set_profiling(int flags);
+    int profiling() const { return profile_flags_; }
+    // Device milliseconds per kernel (setup, generate, trace, shade, shadow) and launch counts.
+    double kernel_ms[5] = {0, 0, 0, 0, 0};
+    uint64_t kernel_launches = 0, iteration_launches = 0;
+    size_t device_bytes() const;
+    int device() const { return device_; }
+    cudaStream_t stream() const { return stream_; }
+    uint64_t bytes_per_path() const;
+
+private:
+    void ensure_shape();
+    void capture(const WfParams& p);
+    WfParams params(const DevScene* scenes, int single, const DevView* views, int n, bool count) const;
+
+    int device_;
+    cudaStream_t stream_;
+    Tuning tuning_;
+    LaunchShape shape_{};
+    bool shape_ok_ = false;
+    PathBuffers pb_{};
+    DeviceBuffer<float4> bufs_[12];
+    DeviceBuffer<uint4> ids_[2];
+    DeviceBuffer<Counters> ctr_;
+    Counters* h_ctr_ = nullptr;
+    Counters last_{};
+    cudaGraphExec_t graph_ = nullptr;
+    WfParams graph_params_{};
+    int graph_iters_ = 0;
+    cudaEvent_t ev_ = nullptr;
+    // continuous mode
+    WfParams cont_params_{};
+    int profile_flags_ = 0;
+    std::vector<cudaEvent_t> prof_ev_;
+    void collect_kernel_times(int iterations);
+};
+
+// The drop-in for photon::GpuRenderer (src/render/gpu_renderer.h:36-75).
+class Renderer {
+public:
+    explicit Renderer(int device);
+    ~Renderer();
+
+    void upload(const pt_scene_desc& d, bool lights_only);
+    void resize(int w, int h);
+    void reset();
+    void render(const pt_camera& cam, const pt_render_settings& rs, int spp);
+    void render_denoised(const pt_camera& cam, const pt_camera& prev, const pt_render_settings& rs, const pt_svgf_settings& sv);
+    void display(const pt_render_settings& rs, int mode, uint32_t* target);
+    void download_image(float* rgb, size_t n);
+    void download_display(uint32_t* out, size_t n);
+    void download_gbuffer(float* albedo4, float* nd4, size_t n);
+    uint32_t* display_buffer() const { return display_.ptr; }
+    void stats(pt_stats* out) const;
+    void set_tuning(const pt_tuning& t);
+    void get_tuning(pt_tuning* t) const;
+
+    void trace_primary(const pt_camera& cam, int w, int h, uint32_t frame, uint32_t seed, float* hits4);
+    void light_picks(const pt_camera& cam, const pt_render_settings& rs, uint32_t frame, int32_t* picks4);
+    void heatmap(const pt_camera& cam, int w, int h, float* out);
+
+    void set_profiling(int flags);
+    void get_profile(pt_profile* out) const;
+    cudaStream_t stream() const { return stream_; }
+
+    void render_views(const pt_view* views, int n);
+    void download_view(int v, float* rgb, size_t n);
+
+    std::string error;
+
+private:
+    void fill_view(DevView& v, const pt_camera& cam, int w, int h, int spp, uint32_t seed, const pt_path_options& po,
+                   uint32_t frame0) const;
+    void render_pass_set(std::vector<DevView>& views, int spp_total, std::vector<int>& spp_each, std::vector<uint32_t>& frame0);
+
+    int device_;
+    cudaStream_t stream_ = nullptr;
+    std::unique_ptr<WavefrontEngine> engine_;
+    DeviceScene scene_;
+    DeviceBuffer<DevScene> scene_table_;
+    int width_ = 0, height_ = 0, samples_ = 0;
+    uint32_t frame_ = 0;
+    float last_ms_ = 0;
+    bool denoised_ = false;
+    DeviceBuffer<float4> accum_, acc_pass_, albedo_, normal_depth_, position_, emission_, color_, denoised_buf_;
+    DeviceBuffer<float> heat_;
+    DeviceBuffer<uint32_t> display_;
+    DeviceBuffer<float4> sample_out_;
+    DeviceBuffer<DevView> d_views_;
+    pt_camera last_camera_{};
+    bool heat_valid_ = false;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    uint64_t sample_cap_ = uint64_t(1) << 26;  // radiance slots per pass (1 GiB)
+    std::unique_ptr<SvgfDenoiser> svgf_;
+    // batched views
+    std::vector<pt_view> batch_views_;
+    std::vector<DeviceBuffer<float4>> batch_accum_;
+    Counters last_ctr_{};
+    pt_profile profile_{};
+    cudaEvent_t acc_ev_[2] = {nullptr, nullptr};
+};
+
+}  // namespace ptw

@@ -1,0 +1,650 @@
+// The wavefront kernels of the path tracer (sm_100a).
+//
+// Photon runs trace_path (src/render/integrator.h:151-263) as one thread per pixel sample. Here the
+// same loop is cut at its ray casts into kernels that each advance every live path by one step:
+//
+//   setup     sizes the iteration from the device counters (no host round trip)
+//   generate  refills free path slots with camera paths (render_sample's RNG, jitter, camera ray)
+//   trace     closest-hit BVH traversal of every live path's ray
+//   shade     emission + MIS, next event estimation (light pick, BSDF eval, shadow ray), BSDF
+//             sampling, Russian roulette; continuing paths and shadow rays are appended to
+//             compacted queues with one atomic per warp (ballot + popc)
+//   shadow    any-hit traversal of the shadow queue; unoccluded contributions are added to their
+//             path (or to a finished path's sample) in the same order as Photon adds them
+//
+// Kernels are persistent: a grid sized to fill the GPU claims 32-path chunks with one atomic per
+// warp until the iteration's count (read from device memory) is exhausted. Compiled with
+// -fmad=false and IEEE division / square root: see pt_math.cuh.
+#include "wavefront.h"
+
+#include "pt_traverse.cuh"
+
+namespace ptw {
+
+namespace {
+
+constexpr uint32_t kFull = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+
+__device__ __forceinline__ uint32_t warp_fetch(uint32_t* ctr) {
+    uint32_t base = 0;
+    if (lane_id() == 0) base = atomicAdd(ctr, 32u);
+    return __shfl_sync(kFull, base, 0);
+}
+
+// Appends the lanes with `pred` to a queue: returns each such lane's slot (one atomic per warp).
+__device__ __forceinline__ uint32_t warp_append(bool pred, uint32_t* ctr) {
+    uint32_t mask = __ballot_sync(kFull, pred);
+    if (mask == 0) return 0;
+    int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (int(lane_id()) == leader) base = atomicAdd(ctr, uint32_t(__popc(mask)));
+    base = __shfl_sync(kFull, base, leader);
+    return base + __popc(mask & ((1u << lane_id()) - 1u));
+}
+
+__device__ __forceinline__ void warp_add_u64(unsigned long long* ctr, uint32_t v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    if (lane_id() == 0 && v) atomicAdd(ctr, (unsigned long long)v);
+}
+
+// Sample slot q of an image -> pixel. Slots run over 8x4 tiles (one warp's camera rays share a
+// tile) and then over the right and bottom remainder strips, so the map is a bijection for any size.
+__device__ __forceinline__ void tile_pixel(uint32_t q, int W, int H, int& x, int& y) {
+    uint32_t tx_n = uint32_t(W) >> 3, ty_n = uint32_t(H) >> 2;
+    uint32_t fw = tx_n * 8, fh = ty_n * 4, full = fw * fh;
+    if (q < full) {
+        uint32_t t = q >> 5, r = q & 31;
+        x = int((t % tx_n) * 8 + (r & 7));
+        y = int((t / tx_n) * 4 + (r >> 3));
+        return;
+    }
+    uint32_t q2 = q - full, rw = uint32_t(W) - fw, cr = rw * fh;
+    if (q2 < cr) {
+        x = int(fw + q2 % rw);
+        y = int(q2 / rw);
+        return;
+    }
+    uint32_t q3 = q2 - cr;
+    x = int(q3 % uint32_t(W));
+    y = int(fh + q3 / uint32_t(W));
+}
+
+// camera_ray (integrator.h:266-280) from a pt_camera laid out as 16 floats.
+__device__ __forceinline__ void camera_ray(const float* c, float px, float py, int width, int height, V2 lens, V3& o, V3& d) {
+    V3 pos{c[0], c[1], c[2]}, fwd{c[4], c[5], c[6]}, right{c[8], c[9], c[10]}, up{c[12], c[13], c[14]};
+    float tan_half_fov = c[3], aspect = c[7], aperture = c[11], focus = c[15];
+    float sx = (2.0f * px / float(width) - 1.0f) * tan_half_fov * aspect;
+    float sy = (1.0f - 2.0f * py / float(height)) * tan_half_fov;
+    d = normalize(fwd + right * sx + up * sy);
+    o = pos;
+    if (aperture > 0) {
+        V3 focus_p = pos + d * (focus / dot(d, fwd));
+        V2 l = concentric_disk(lens) * aperture;
+        o = pos + right * l.x + up * l.y;
+        d = normalize(focus_p - o);
+    }
+}
+
+__device__ __forceinline__ const DevScene& scene_for(const WfParams& P, int view) {
+    return P.single_scene >= 0 ? P.scenes[P.single_scene] : P.scenes[P.views[view].scene];
+}
+
+__device__ __forceinline__ float clamp_contribution(V3& c, int depth, float clamp) {
+    if (depth > 0 && clamp > 0) {
+        float l = luminance(c);
+        if (l > clamp) c = c * (clamp / l);
+    }
+    return 0;
+}
+
+__device__ __forceinline__ int find_view(const DevView* views, int n, unsigned long long w) {
+    int lo = 0, hi = n;
+    while (lo + 1 < hi) {
+        int mid = (lo + hi) >> 1;
+        if (views[mid].work_begin <= w) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// ---- setup ------------------------------------------------------------------------------------------
+__global__ void k_setup(Counters* c, uint32_t capacity) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t p = c->parity ^ 1u;
+    c->parity = p;
+    uint32_t cnt = c->count[p];
+    unsigned long long remaining = c->work_total > c->work_next ? c->work_total - c->work_next : 0ull;
+    uint32_t room = capacity > cnt ? capacity - cnt : 0u;
+    uint32_t n = remaining < room ? uint32_t(remaining) : room;
+    c->gen_base = cnt;
+    c->gen_n = n;
+    c->work_base = c->work_next;
+    c->work_next += n;
+    c->count[p] = cnt + n;
+    c->count[p ^ 1u] = 0;
+    c->shadow_rays += c->shadow_count;
+    c->shadow_count = 0;
+    c->rays += cnt + n;
+    c->fetch[0] = c->fetch[1] = c->fetch[2] = c->fetch[3] = 0;
+    if (cnt + n > 0) c->iterations++;
+}
+
+// ---- generate: render_sample's camera path (pixel.h:18-24) --------------------------------------------
+__global__ void __launch_bounds__(256) k_generate(const __grid_constant__ WfParams P) {
+    Counters* c = P.ctr;
+    const uint32_t p = c->parity, base = c->gen_base, n = c->gen_n;
+    const unsigned long long wb = c->work_base;
+    for (;;) {
+        uint32_t k0 = warp_fetch(&c->fetch[0]);
+        if (k0 >= n) break;
+        uint32_t k = k0 + lane_id();
+        if (k >= n) continue;
+        unsigned long long wg = wb + k;
+        int vi = find_view(P.views, P.num_views, wg);
+        const DevView& v = P.views[vi];
+        uint32_t local = uint32_t(wg - v.work_begin);
+        uint32_t npix = uint32_t(v.width) * uint32_t(v.height);
+        uint32_t s = local / npix, q = local - s * npix;
+        int x, y;
+        tile_pixel(q, v.width, v.height, x, y);
+        uint32_t pixel = uint32_t(y) * uint32_t(v.width) + uint32_t(x);
+        Rng rng = pixel_rng(pixel, v.seed, v.frame0 + s);
+        V2 jitter = rng_next2(rng);
+        V2 lens = rng_next2(rng);
+        V3 o, d;
+        camera_ray(v.cam, float(x) + jitter.x, float(y) + jitter.y, v.width, v.height, lens, o, d);
+        uint32_t slot = base + k;
+        P.pb.o[p][slot] = make_float4(o.x, o.y, o.z, 0.0f);
+        P.pb.d[p][slot] = make_float4(d.x, d.y, d.z, __uint_as_float(1u << 16));  // depth 0, prev_delta
+        P.pb.beta[p][slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        P.pb.lr[p][slot] = make_float4(0.0f, 0.0f, __uint_as_float(uint32_t(rng.state)), __uint_as_float(uint32_t(rng.state >> 32)));
+        P.pb.id[p][slot] = make_uint4(uint32_t(vi), local, pixel, s);
+    }
+}
+
+// ---- trace: closest hit (traverse.h:140-142) -------------------------------------------------------
+template <bool Count>
+__global__ void __launch_bounds__(256) k_trace(const __grid_constant__ WfParams P) {
+    extern __shared__ int smem_stack[];
+    int* stack = smem_stack + threadIdx.x;
+    Counters* c = P.ctr;
+    const uint32_t p = c->parity, n = c->count[p];
+    TraversalCounters tc{0, 0};
+    for (;;) {
+        uint32_t i0 = warp_fetch(&c->fetch[1]);
+        if (i0 >= n) break;
+        uint32_t i = i0 + lane_id();
+        if (i < n) {
+            float4 o4 = P.pb.o[p][i], d4 = P.pb.d[p][i];
+            int view = P.single_scene >= 0 ? 0 : int(P.pb.id[p][i].x);
+            const DevScene& s = scene_for(P, view);
+            Hit h{kInf, -1, 0.0f, 0.0f};
+            traverse<false, Count>(s, xyz(o4), xyz(d4), kInf, h, stack, blockDim.x, &tc);
+            P.pb.hit[i] = make_float4(h.t, __int_as_float(h.tri), h.u, h.v);
+        }
+    }
+    if (Count) {
+        warp_add_u64(&c->node_visits, tc.nodes);
+        warp_add_u64(&c->tri_tests, tc.tris);
+    }
+}
+
+// ---- shade: one vertex of trace_path (integrator.h:158-262) -----------------------------------------
+__global__ void __launch_bounds__(256) k_shade(const __grid_constant__ WfParams P) {
+    Counters* c = P.ctr;
+    const uint32_t p = c->parity, q = p ^ 1u, n = c->count[p];
+    for (;;) {
+        uint32_t i0 = warp_fetch(&c->fetch[2]);
+        if (i0 >= n) break;
+        uint32_t i = i0 + lane_id();
+        bool active = i < n;
+        bool cont = false, shadow = false;
+        // Path state.
+        V3 ro{0, 0, 0}, rd{0, 0, 0}, beta{0, 0, 0}, L{0, 0, 0}, sh_o{0, 0, 0}, sh_d{0, 0, 0}, sh_c{0, 0, 0};
+        float prev_pdf = 0, sh_tmax = 0;
+        uint32_t flags = 0;
+        uint4 id = make_uint4(0, 0, 0, 0);
+        Rng rng{0, 1};
+        if (active) {
+            float4 o4 = P.pb.o[p][i], d4 = P.pb.d[p][i], b4 = P.pb.beta[p][i], l4 = P.pb.lr[p][i], h4 = P.pb.hit[i];
+            id = P.pb.id[p][i];
+            const DevView& v = P.views[id.x];
+            const DevScene& s = scene_for(P, id.x);
+            ro = xyz(o4);
+            rd = xyz(d4);
+            prev_pdf = o4.w;
+            flags = __float_as_uint(d4.w);
+            int depth = int(flags & 0xffffu);
+            bool prev_delta = (flags >> 16) & 1u;
+            beta = xyz(b4);
+            L = V3{b4.w, l4.x, l4.y};
+            rng.state = uint64_t(__float_as_uint(l4.z)) | (uint64_t(__float_as_uint(l4.w)) << 32);
+            rng.inc = (uint64_t(id.z) << 1u) | 1u;
+            int tri = __float_as_int(h4.y);
+            bool gbuf = v.gbuffer && id.w == 0 && depth == 0;
+            if (tri < 0) {
+                // Miss: the environment, weighted against light sampling (integrator.h:159-177).
+                V3 le = env_radiance(s, rd);
+                float w = (prev_delta || s.p_env <= 0) ? 1.0f : power_heuristic(prev_pdf, env_pdf(s, rd));
+                V3 cc = beta * le * w;
+                clamp_contribution(cc, depth, v.clamp);
+                L = L + cc;
+                if (gbuf) {
+                    V3 pos = ro + rd * 1e4f;
+                    v.g_albedo[id.z] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+                    v.g_normal_depth[id.z] = make_float4(-rd.x, -rd.y, -rd.z, 0.0f);
+                    if (v.g_position) v.g_position[id.z] = make_float4(pos.x, pos.y, pos.z, -1.0f);
+                    if (v.g_emission) v.g_emission[id.z] = make_float4(le.x, le.y, le.z, 1.0f);
+                }
+            } else {
+                Interaction it = surface_at(s, ro, rd, h4.x, tri, h4.z, h4.w);
+                V3 wo_world = -rd;
+                if (!is_black(it.emission)) {
+                    float w = 1.0f;
+                    if (!prev_delta) w = power_heuristic(prev_pdf, emissive_pdf(s, tri, it.emissive_entry, rd, h4.x));
+                    V3 cc = beta * it.emission * w;
+                    clamp_contribution(cc, depth, v.clamp);
+                    L = L + cc;
+                }
+                Bsdf bsdf = make_bsdf(it.params);
+                if (gbuf) {
+                    V3 alb = bsdf_albedo(bsdf);
+                    v.g_albedo[id.z] = make_float4(alb.x, alb.y, alb.z, 1.0f);
+                    v.g_normal_depth[id.z] = make_float4(it.ns.x, it.ns.y, it.ns.z, h4.x);
+                    if (v.g_position) v.g_position[id.z] = make_float4(it.p.x, it.p.y, it.p.z, float(it.material));
+                    if (v.g_emission) v.g_emission[id.z] = make_float4(it.emission.x, it.emission.y, it.emission.z, 1.0f);
+                }
+                if (depth + 1 < v.max_depth) {
+                    V3 wo = to_local(it.frame, wo_world);
+                    bool nee = v.nee && s.has_lights && samples_lights(bsdf);
+                    if (nee) {
+                        float ug = rng_next(rng);
+                        V2 ul = rng_next2(rng);
+                        float uk = rng_next(rng);
+                        LightSample ls = sample_light(s, it.p, ug, ul, uk, nullptr);
+                        if (ls.pdf > 0 && !is_black(ls.radiance)) {
+                            V3 wi = to_local(it.frame, ls.wi);
+                            float pdf_b;
+                            V3 f = bsdf_eval_pdf(bsdf, wo, wi, &pdf_b);
+                            if (!is_black(f)) {
+                                sh_o = offset_ray(it.p, dot(ls.wi, it.ng) > 0 ? it.ng : -it.ng);
+                                sh_d = ls.wi;
+                                sh_tmax = ls.dist == kInf ? kInf : ls.dist * (1.0f - 1e-4f);
+                                float w = ls.delta ? 1.0f : power_heuristic(ls.pdf, pdf_b);
+                                sh_c = beta * f * fabsf(wi.z) * ls.radiance * (w / ls.pdf);
+                                clamp_contribution(sh_c, depth, v.clamp);
+                                shadow = true;
+                            }
+                        }
+                    }
+                    float u_lobe = rng_next(rng);
+                    V2 u = rng_next2(rng);
+                    float u_sub = rng_next(rng);
+                    BsdfSample bs = bsdf_sample(bsdf, wo, u_lobe, u, u_sub);
+                    if (bs.valid) {
+                        beta = beta * (bs.f * (fabsf(bs.wi.z) / bs.pdf));
+                        if (is_finite(beta) && !is_black(beta)) {
+                            V3 wi_world = to_world(it.frame, bs.wi);
+                            float side = dot(wi_world, it.ng) * dot(wo_world, it.ng);
+                            if (!(bs.transmitted ? side >= 0 : side <= 0)) {
+                                prev_pdf = bs.pdf;
+                                ro = offset_ray(it.p, dot(wi_world, it.ng) > 0 ? it.ng : -it.ng);
+                                rd = normalize(wi_world);
+                                cont = true;
+                                if (depth + 1 >= v.rr_depth) {
+                                    float qq = fmaxf(0.05f, 1.0f - max_component(beta));
+                                    if (rng_next(rng) < qq) cont = false;
+                                    else beta = beta * (1.0f / (1.0f - qq));
+                                }
+                                flags = uint32_t(depth + 1) | ((nee ? 0u : 1u) << 16);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        // Continuing paths move to the other buffer, compacted.
+        uint32_t slot = warp_append(cont, &c->count[q]);
+        if (cont) {
+            P.pb.o[q][slot] = make_float4(ro.x, ro.y, ro.z, prev_pdf);
+            P.pb.d[q][slot] = make_float4(rd.x, rd.y, rd.z, __uint_as_float(flags));
+            P.pb.beta[q][slot] = make_float4(beta.x, beta.y, beta.z, L.x);
+            P.pb.lr[q][slot] = make_float4(L.y, L.z, __uint_as_float(uint32_t(rng.state)), __uint_as_float(uint32_t(rng.state >> 32)));
+            P.pb.id[q][slot] = id;
+        } else if (active) {
+            const DevView& v = P.views[id.x];
+            v.sample_out[id.y] = make_float4(L.x, L.y, L.z, 0.0f);
+        }
+        // Shadow rays: target the continuing slot, or the finished sample.
+        uint32_t qs = warp_append(shadow, &c->shadow_count);
+        if (shadow) {
+            P.pb.sh0[qs] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_tmax);
+            P.pb.sh1[qs] = make_float4(sh_d.x, sh_d.y, sh_d.z, __uint_as_float(cont ? slot : id.y));
+            P.pb.sh2[qs] = make_float4(sh_c.x, sh_c.y, sh_c.z, __uint_as_float(id.x | (cont ? 0u : 0x80000000u)));
+        }
+        // Progress of views that count finished paths (the request server).
+        bool finished = active && !cont;
+        if (P.num_views > 1 || P.views[0].done_counter) {
+            uint32_t key = finished ? id.x : 0xffffffffu;
+            uint32_t peers = __match_any_sync(kFull, key);
+            if (finished && int(lane_id()) == __ffs(peers) - 1) {
+                unsigned long long* dc = P.views[id.x].done_counter;
+                if (dc) atomicAdd(dc, (unsigned long long)__popc(peers));
+            }
+        }
+    }
+}
+
+// ---- shadow: any hit (traverse.h:144-147) --------------------------------------------------------------
+template <bool Count>
+__global__ void __launch_bounds__(256) k_shadow(const __grid_constant__ WfParams P) {
+    extern __shared__ int smem_stack[];
+    int* stack = smem_stack + threadIdx.x;
+    Counters* c = P.ctr;
+    const uint32_t q = c->parity ^ 1u, n = c->shadow_count;
+    TraversalCounters tc{0, 0};
+    for (;;) {
+        uint32_t i0 = warp_fetch(&c->fetch[3]);
+        if (i0 >= n) break;
+        uint32_t i = i0 + lane_id();
+        if (i >= n) continue;
+        float4 a = P.pb.sh0[i], b = P.pb.sh1[i], cc = P.pb.sh2[i];
+        uint32_t tag = __float_as_uint(cc.w);
+        uint32_t view = tag & 0x7fffffffu;
+        const DevScene& s = scene_for(P, int(view));
+        Hit h{kInf, -1, 0.0f, 0.0f};
+        bool occ = traverse<true, Count>(s, xyz(a), xyz(b), a.w, h, stack, blockDim.x, &tc);
+        if (!occ) {
+            uint32_t target = __float_as_uint(b.w);
+            if (tag & 0x80000000u) {
+                float4* so = P.views[view].sample_out + target;
+                float4 l = *so;
+                *so = make_float4(l.x + cc.x, l.y + cc.y, l.z + cc.z, l.w);
+            } else {
+                float4 b4 = P.pb.beta[q][target], l4 = P.pb.lr[q][target];
+                b4.w = b4.w + cc.x;
+                l4.x = l4.x + cc.y;
+                l4.y = l4.y + cc.z;
+                P.pb.beta[q][target] = b4;
+                P.pb.lr[q][target] = l4;
+            }
+        }
+    }
+    if (Count) {
+        warp_add_u64(&c->shadow_node_visits, tc.nodes);
+        warp_add_u64(&c->shadow_tri_tests, tc.tris);
+    }
+}
+
+// ---- accumulate: CpuRenderer's per-pixel sum in sample order (cpu_renderer.cpp:28-31) ------------------
+__global__ void k_accumulate(const DevView* vp, int first, int last) {
+    const DevView& v = *vp;
+    uint32_t npix = uint32_t(v.width) * uint32_t(v.height);
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npix) return;
+    int x, y;
+    tile_pixel(q, v.width, v.height, x, y);
+    uint32_t pix = uint32_t(y) * uint32_t(v.width) + uint32_t(x);
+    float4 acc = first ? make_float4(0, 0, 0, 0) : v.acc_pass[pix];
+    for (int s = 0; s < v.spp; s++) {
+        float4 l4 = v.sample_out[size_t(s) * npix + q];
+        V3 l = xyz(l4);
+        // render_sample's guard (pixel.h:26-27).
+        if (!is_finite(l) || l.x < 0 || l.y < 0 || l.z < 0) l = v3(0);
+        acc.x = acc.x + l.x;
+        acc.y = acc.y + l.y;
+        acc.z = acc.z + l.z;
+        float lum = luminance(l);
+        acc.w = acc.w + lum * lum;
+        if (v.realtime && s == 0 && v.g_color) v.g_color[pix] = make_float4(l.x, l.y, l.z, 1.0f);
+    }
+    if (last) {
+        float4 a = v.accum[pix];
+        a.x = a.x + acc.x;
+        a.y = a.y + acc.y;
+        a.z = a.z + acc.z;
+        a.w = a.w + acc.w;
+        v.accum[pix] = a;
+    } else {
+        v.acc_pass[pix] = acc;
+    }
+}
+
+// ---- probes ----------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_trace_primary(const DevScene* sp, CameraArg cam, int w, int h, uint32_t frame, uint32_t seed,
+                                                      float4* out) {
+    extern __shared__ int smem_stack[];
+    int x = blockIdx.x * 16 + (threadIdx.x & 15), y = blockIdx.y * 8 + (threadIdx.x >> 4);
+    if (x >= w || y >= h) return;
+    const DevScene& s = *sp;
+    uint32_t pixel = uint32_t(y) * uint32_t(w) + uint32_t(x);
+    Rng rng = pixel_rng(pixel, seed, frame);
+    V2 jitter = rng_next2(rng);
+    V2 lens = rng_next2(rng);
+    V3 o, d;
+    camera_ray(cam.c, float(x) + jitter.x, float(y) + jitter.y, w, h, lens, o, d);
+    Hit hit{kInf, -1, 0.0f, 0.0f};
+    TraversalCounters tc{0, 0};
+    traverse<false, false>(s, o, d, kInf, hit, smem_stack + threadIdx.x, blockDim.x, &tc);
+    out[pixel] = make_float4(hit.t, __int_as_float(hit.tri), hit.u, hit.v);
+}
+
+__global__ void __launch_bounds__(128) k_heatmap(const DevScene* sp, CameraArg cam, int w, int h, float* out) {
+    extern __shared__ int smem_stack[];
+    int x = blockIdx.x * 16 + (threadIdx.x & 15), y = blockIdx.y * 8 + (threadIdx.x >> 4);
+    if (x >= w || y >= h) return;
+    V3 o, d;
+    camera_ray(cam.c, float(x) + 0.5f, float(y) + 0.5f, w, h, V2{0.5f, 0.5f}, o, d);
+    Hit hit{kInf, -1, 0.0f, 0.0f};
+    TraversalCounters tc{0, 0};
+    traverse<false, true>(*sp, o, d, kInf, hit, smem_stack + threadIdx.x, blockDim.x, &tc);
+    out[size_t(y) * size_t(w) + size_t(x)] = float(tc.nodes);
+}
+
+// The light pick of the first vertex of each pixel's sample (integrator.h:199-209).
+__global__ void __launch_bounds__(128) k_light_picks(const DevScene* sp, const DevView* vp, int4* out) {
+    extern __shared__ int smem_stack[];
+    const DevView& v = *vp;
+    int x = blockIdx.x * 16 + (threadIdx.x & 15), y = blockIdx.y * 8 + (threadIdx.x >> 4);
+    if (x >= v.width || y >= v.height) return;
+    const DevScene& s = *sp;
+    uint32_t pixel = uint32_t(y) * uint32_t(v.width) + uint32_t(x);
+    int4 res = make_int4(-1, -1, -1, 0);
+    Rng rng = pixel_rng(pixel, v.seed, v.frame0);
+    V2 jitter = rng_next2(rng);
+    V2 lens = rng_next2(rng);
+    V3 o, d;
+    camera_ray(v.cam, float(x) + jitter.x, float(y) + jitter.y, v.width, v.height, lens, o, d);
+    Hit hit{kInf, -1, 0.0f, 0.0f};
+    TraversalCounters tc{0, 0};
+    if (traverse<false, false>(s, o, d, kInf, hit, smem_stack + threadIdx.x, blockDim.x, &tc) && 1 < v.max_depth) {
+        Interaction it = surface_at(s, o, d, hit.t, hit.tri, hit.u, hit.v);
+        Bsdf bsdf = make_bsdf(it.params);
+        bool nee = v.nee && s.has_lights && samples_lights(bsdf);
+        if (nee) {
+            float ug = rng_next(rng);
+            V2 ul = rng_next2(rng);
+            float uk = rng_next(rng);
+            LightPick pk;
+            sample_light(s, it.p, ug, ul, uk, &pk);
+            res = make_int4(pk.group, pk.index, pk.bin, 1);
+        }
+    }
+    out[pixel] = res;
+}
+
+// ---- display (gpu_renderer.cu:108-175 semantics; color.h:8-41) ---------------------------------------------
+__device__ float srgb_to_linear_d(float c) { return c <= 0.04045f ? c / 12.92f : powf((c + 0.055f) / 1.055f, 2.4f); }
+__device__ float linear_to_srgb_d(float c) {
+    c = saturate(c);
+    return c <= 0.0031308f ? c * 12.92f : 1.055f * powf(c, 1.0f / 2.4f) - 0.055f;
+}
+__device__ V3 aces_fitted_d(V3 c) {
+    V3 v{0.59719f * c.x + 0.35458f * c.y + 0.04823f * c.z, 0.07600f * c.x + 0.90834f * c.y + 0.01566f * c.z,
+         0.02840f * c.x + 0.13383f * c.y + 0.83777f * c.z};
+    V3 a = v * (v + v3(0.0245786f)) - v3(0.000090537f);
+    V3 b = v * (v * 0.983729f + v3(0.4329510f)) + v3(0.238081f);
+    v = V3{a.x / b.x, a.y / b.y, a.z / b.z};
+    V3 r{1.60475f * v.x - 0.53108f * v.y - 0.07367f * v.z, -0.10208f * v.x + 1.10813f * v.y - 0.00605f * v.z,
+         -0.00327f * v.x - 0.07276f * v.y + 1.07602f * v.z};
+    return V3{clampf(r.x, 0.0f, 1.0f), clampf(r.y, 0.0f, 1.0f), clampf(r.z, 0.0f, 1.0f)};
+}
+__device__ V3 tone_map_d(V3 c, float exposure, int op) {
+    c = c * exposure;
+    if (op == 1) return aces_fitted_d(c);
+    if (op == 2) return V3{c.x / (1.0f + c.x), c.y / (1.0f + c.y), c.z / (1.0f + c.z)};
+    return V3{clampf(c.x, 0.0f, 1.0f), clampf(c.y, 0.0f, 1.0f), clampf(c.z, 0.0f, 1.0f)};
+}
+__device__ uint32_t quantize_d(float v) { return uint32_t(saturate(v) * 255.0f + 0.5f); }
+__device__ uint32_t pack_rgba8_d(V3 c) {
+    return quantize_d(linear_to_srgb_d(c.x)) | (quantize_d(linear_to_srgb_d(c.y)) << 8) | (quantize_d(linear_to_srgb_d(c.z)) << 16) |
+           0xFF000000u;
+}
+__device__ V3 heat_color_d(float t) {
+    t = saturate(t);
+    V3 c0{0.05f, 0.05f, 0.35f}, c1{0.0f, 0.6f, 0.4f}, c2{0.95f, 0.85f, 0.1f}, c3{0.85f, 0.1f, 0.05f};
+    if (t < 1.0f / 3) return lerp(c0, c1, t * 3);
+    if (t < 2.0f / 3) return lerp(c1, c2, t * 3 - 1);
+    return lerp(c2, c3, t * 3 - 2);
+}
+__global__ void k_display(DisplayParams p, const float4* accum, const float4* denoised, const float4* albedo, const float4* normal_depth,
+                          const float4* variance, const float* heat, uint32_t* out) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= p.w || y >= p.h) return;
+    int i = y * p.w + x;
+    V3 c;
+    switch (p.mode) {
+        case 1: c = xyz(albedo[i]); break;
+        case 2: {
+            float4 nd = normal_depth[i];
+            c = nd.w > 0 ? xyz(nd) * 0.5f + v3(0.5f) : v3(0);
+            break;
+        }
+        case 3: {
+            float d = normal_depth[i].w;
+            c = d > 0 ? v3(1.0f - saturate(d / p.max_depth)) : v3(0);
+            break;
+        }
+        case 4: {
+            float var;
+            if (p.denoised) {
+                var = variance ? variance[i].w : 0.0f;
+            } else {
+                float4 a = accum[i];
+                float mean = luminance(xyz(a)) * p.inv_samples;
+                var = p.samples > 1 ? fmaxf(0.0f, a.w * p.inv_samples - mean * mean) / (p.samples - 1) : 0.0f;
+            }
+            float t = sqrtf(var);
+            c = v3(t / (1.0f + t));
+            break;
+        }
+        case 5: c = heat_color_d(heat[i] * p.heat_scale); break;
+        default:
+            c = p.denoised ? xyz(denoised[i]) : xyz(accum[i]) * p.inv_samples;
+            c = tone_map_d(c, p.exposure, p.tonemap);
+            break;
+    }
+    if (p.mode != 0 && p.mode != 1) c = V3{srgb_to_linear_d(c.x), srgb_to_linear_d(c.y), srgb_to_linear_d(c.z)};
+    out[i] = pack_rgba8_d(c);
+}
+
+int g_smem_trace = 0;
+
+}  // namespace
+
+cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, LaunchShape* out) {
+    cudaDeviceProp prop;
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return e;
+    out->sms = prop.multiProcessorCount;
+    int nb = 0;
+    out->gen_block = 256;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_generate, 256, 0);
+    if (e != cudaSuccess) return e;
+    out->gen_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
+    out->trace_block = trace_block;
+    size_t smem = size_t(kSmemStack) * trace_block * sizeof(int);
+    e = cudaFuncSetAttribute(k_trace<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_trace<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_shadow<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_shadow<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace<false>, trace_block, smem);
+    if (e != cudaSuccess) return e;
+    out->trace_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
+    out->shadow_block = trace_block;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shadow<false>, trace_block, smem);
+    if (e != cudaSuccess) return e;
+    out->shadow_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
+    out->shade_block = shade_block;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade, shade_block, 0);
+    if (e != cudaSuccess) return e;
+    out->shade_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
+    g_smem_trace = int(smem);
+    return cudaSuccess;
+}
+
+cudaError_t wf_iteration(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, cudaEvent_t* ev) {
+    size_t smem = size_t(kSmemStack) * ls.trace_block * sizeof(int);
+    if (ev) cudaEventRecord(ev[0], stream);
+    k_setup<<<1, 32, 0, stream>>>(p.ctr, p.pb.capacity);
+    if (ev) cudaEventRecord(ev[1], stream);
+    k_generate<<<ls.gen_grid, ls.gen_block, 0, stream>>>(p);
+    if (ev) cudaEventRecord(ev[2], stream);
+    if (p.count_work) k_trace<true><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
+    else k_trace<false><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
+    if (ev) cudaEventRecord(ev[3], stream);
+    k_shade<<<ls.shade_grid, ls.shade_block, 0, stream>>>(p);
+    if (ev) cudaEventRecord(ev[4], stream);
+    if (p.count_work) k_shadow<true><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
+    else k_shadow<false><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
+    if (ev) cudaEventRecord(ev[5], stream);
+    return cudaGetLastError();
+}
+
+cudaError_t wf_accumulate(const DevView* d_view, const DevView& h_view, int first_pass, int last_pass, cudaStream_t stream) {
+    uint32_t npix = uint32_t(h_view.width) * uint32_t(h_view.height);
+    if (npix == 0) return cudaSuccess;
+    k_accumulate<<<(npix + 255) / 256, 256, 0, stream>>>(d_view, first_pass, last_pass);
+    return cudaGetLastError();
+}
+
+cudaError_t wf_trace_primary(const DevScene* scene, const float* cam16, int w, int h, uint32_t frame, uint32_t seed, float4* out,
+                             cudaStream_t stream) {
+    CameraArg c;
+    for (int i = 0; i < 16; i++) c.c[i] = cam16[i];
+    dim3 grid((w + 15) / 16, (h + 7) / 8);
+    size_t smem = size_t(kSmemStack) * 128 * sizeof(int);
+    k_trace_primary<<<grid, 128, smem, stream>>>(scene, c, w, h, frame, seed, out);
+    return cudaGetLastError();
+}
+
+cudaError_t wf_light_picks(const DevScene* scene, const DevView* view, int4* out, int w, int h, cudaStream_t stream) {
+    dim3 grid((w + 15) / 16, (h + 7) / 8);
+    size_t smem = size_t(kSmemStack) * 128 * sizeof(int);
+    k_light_picks<<<grid, 128, smem, stream>>>(scene, view, out);
+    return cudaGetLastError();
+}
+
+cudaError_t wf_heatmap(const DevScene* scene, const float* cam16, int w, int h, float* out, cudaStream_t stream) {
+    CameraArg c;
+    for (int i = 0; i < 16; i++) c.c[i] = cam16[i];
+    dim3 grid((w + 15) / 16, (h + 7) / 8);
+    size_t smem = size_t(kSmemStack) * 128 * sizeof(int);
+    k_heatmap<<<grid, 128, smem, stream>>>(scene, c, w, h, out);
+    return cudaGetLastError();
+}
+
+cudaError_t wf_display(const DisplayParams& p, const float4* accum, const float4* denoised, const float4* albedo,
+                       const float4* normal_depth, const float4* variance, const float* heat, uint32_t* out, cudaStream_t stream) {
+    dim3 block(16, 8), grid((p.w + 15) / 16, (p.h + 7) / 8);
+    k_display<<<grid, block, 0, stream>>>(p, accum, denoised, albedo, normal_depth, variance, heat, out);
+    return cudaGetLastError();
+}
+
+}  // namespace ptw

@@ -1,0 +1,113 @@
+// Host-side interface of the wavefront kernels (wavefront.cu): the device structures shared by the
+// kernels and the renderer, and the launch wrappers.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pt_types.h"
+
+namespace ptw {
+
+// One unit of batched work: a camera over an image, spp samples per pixel starting at sample index
+// frame0. Every (sample, pixel) pair is one path; paths of all views share the path pool.
+struct DevView {
+    float cam[16];            // pt_camera: position, tan_half_fov, forward, aspect, right, aperture, up, focus
+    int width, height, spp, scene;
+    uint32_t seed, frame0;
+    int max_depth, rr_depth;
+    int nee;
+    float clamp;
+    int gbuffer;              // 1: sample 0 writes the first-hit G-buffer
+    int realtime;             // 1: the accumulate step also writes `color` (sample 0)
+    unsigned long long work_begin, work_count;
+    float4* sample_out;       // work_count radiance values, indexed by (sample * pixels + tile slot)
+    float4* accum;            // rgb sum + luminance^2 sum per pixel
+    float4* acc_pass;         // running per-call sum across passes (may be null for single-pass calls)
+    float4* g_albedo;
+    float4* g_normal_depth;
+    float4* g_position;
+    float4* g_emission;
+    float4* g_color;
+    unsigned long long* done_counter;  // optional: paths finished (for serving progress)
+};
+
+// Device counters of one wavefront run. The kernels read the iteration's sizes from here, so a
+// bounce iteration is a fixed launch sequence that a CUDA graph can replay.
+struct Counters {
+    uint32_t parity;                 // buffer holding this iteration's paths
+    uint32_t count[2];               // paths in each buffer
+    uint32_t shadow_count;
+    uint32_t gen_base, gen_n;        // slots filled by this iteration's generate step
+    uint32_t fetch[4];               // work-claim counters of generate / trace / shade / shadow
+    uint32_t overflow;
+    uint32_t iterations;
+    unsigned long long work_base, work_next, work_total;
+    unsigned long long rays, shadow_rays, paths_done;
+    unsigned long long node_visits, tri_tests;
+    unsigned long long shadow_node_visits, shadow_tri_tests;
+};
+
+struct PathBuffers {
+    float4* o[2];      // (origin, prev_pdf)
+    float4* d[2];      // (direction, flags: depth | prev_delta << 16)
+    float4* beta[2];   // (beta, L.x)
+    float4* lr[2];     // (L.y, L.z, rng state lo, rng state hi)
+    uint4* id[2];      // (view, local work index, pixel, sample in pass)
+    float4* hit;       // (t, tri, u, v)
+    float4* sh0;       // shadow queue: (origin, tmax)
+    float4* sh1;       // (direction, target)
+    float4* sh2;       // (contribution, view | terminal flag)
+    uint32_t capacity;
+};
+
+struct WfParams {
+    const DevScene* scenes;
+    const DevView* views;
+    int num_views;
+    int single_scene;          // >= 0: every view uses this scene slot
+    PathBuffers pb;
+    Counters* ctr;
+    int count_work;            // 1: count node visits / triangle tests (stats runs)
+};
+
+// A camera passed by value to the probe kernels (pt_camera as 16 floats).
+struct CameraArg {
+    float c[16];
+};
+
+struct LaunchShape {
+    int sms;
+    int gen_grid, gen_block;
+    int trace_grid, trace_block;
+    int shade_grid, shade_block;
+    int shadow_grid, shadow_block;
+};
+
+// Fills grid sizes from the occupancy of each kernel on `device` (block sizes as requested).
+cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, LaunchShape* out);
+// One bounce iteration: setup, generate, trace, shade, shadow. With `events` (6 entries), an event
+// is recorded before the first kernel and after each of the five.
+cudaError_t wf_iteration(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, cudaEvent_t* events = nullptr);
+constexpr int kKernelsPerIteration = 5;
+// Sums the samples of every pixel of a view in sample order (after a pass).
+cudaError_t wf_accumulate(const DevView* d_view, const DevView& h_view, int first_pass, int last_pass, cudaStream_t stream);
+
+// Probes (same device functions as the wavefront).
+cudaError_t wf_trace_primary(const DevScene* scene, const float* cam16, int w, int h, uint32_t frame, uint32_t seed,
+                             float4* out, cudaStream_t stream);
+cudaError_t wf_light_picks(const DevScene* scene, const DevView* view, int4* out, int w, int h, cudaStream_t stream);
+cudaError_t wf_heatmap(const DevScene* scene, const float* cam16, int w, int h, float* out, cudaStream_t stream);
+
+struct DisplayParams {
+    int w, h, mode;
+    float exposure;
+    int tonemap;
+    float inv_samples, samples, max_depth, heat_scale;
+    int denoised;
+};
+cudaError_t wf_display(const DisplayParams& p, const float4* accum, const float4* denoised, const float4* albedo,
+                       const float4* normal_depth, const float4* variance, const float* heat, uint32_t* out,
+                       cudaStream_t stream);
+
+}  // namespace ptw

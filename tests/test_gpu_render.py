@@ -1,0 +1,179 @@
+"""Parity of the CUDA wavefront with the oracle, through the C ABI (gpu).
+
+Bars (from the contract of this path): primary closest-hit triangle indices and the first
+vertex's light picks are bit-exact; images agree within 1e-3 * max(1, max channel) per pixel
+(Photon's own comparison, tests/test_gpu.cpp:58-68) on >= 99.9% of the pixels, with means within
+1%. Tolerances are written next to each check."""
+import numpy as np
+import pytest
+
+from conftest import pixel_agreement
+from oracle import oracle as O
+from photon_b200 import abi, native
+import scenes
+
+pytestmark = pytest.mark.gpu
+
+SCENES = ["cornell", "materials", "glass", "box", "terrain"]
+PIXEL_FRACTION = 0.999   # >= 99.9% of pixels within the 1e-3 relative tolerance
+MEAN_REL = 0.01          # means within 1%
+
+
+@pytest.fixture(scope="module")
+def renderer():
+    r = native.Renderer()
+    yield r
+    r.close()
+
+
+def _settings(name, w, h, **kw):
+    depth = 12 if name == "terrain" else 8
+    return abi.render_settings(w, h, max_depth=kw.pop("max_depth", depth), **kw)
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_primary_hits_bit_exact(renderer, name):
+    desc, camf, keep = scenes.scene(name)
+    w, h = (320, 180) if name == "terrain" else (96, 54)
+    cam = camf(w / h)
+    renderer.upload(desc)
+    for frame, seed in ((0, 0), (5, 7)):
+        gpu = renderer.trace_primary(cam, w, h, frame, seed)
+        ref = O.orc_trace_primary(desc, cam, w, h, frame, seed)
+        assert np.array_equal(O.hits_tri(gpu), O.hits_tri(ref))          # triangle indices: exact
+        assert np.array_equal(gpu.view(np.uint32), ref.view(np.uint32))  # t, u, v: exact bits
+    assert (O.hits_tri(gpu) >= 0).mean() > 0.3
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_light_picks_bit_exact(renderer, name):
+    desc, camf, keep = scenes.scene(name)
+    w, h = (320, 180) if name == "terrain" else (96, 54)
+    cam = camf(w / h)
+    rs = _settings(name, w, h, seed=3)
+    renderer.upload(desc)
+    for frame in (0, 9):
+        gpu = renderer.light_picks(cam, rs, frame)
+        ref = O.orc_light_picks(desc, cam, rs, frame)
+        assert np.array_equal(gpu, ref)
+    assert gpu[..., 3].mean() > 0.2  # the check exercised NEE
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_heatmap_matches_node_visits(renderer, name):
+    desc, camf, keep = scenes.scene(name)
+    w, h = 64, 36
+    cam = camf(w / h)
+    renderer.upload(desc)
+    assert np.array_equal(renderer.heatmap(cam, w, h), O.orc_heatmap(desc, cam, w, h))
+
+
+@pytest.mark.parametrize("name,w,h,spp", [("cornell", 96, 54, 64), ("materials", 96, 54, 64), ("glass", 96, 54, 64),
+                                          ("box", 128, 128, 64), ("terrain", 192, 108, 16)])
+def test_images_agree_with_oracle(renderer, name, w, h, spp):
+    desc, camf, keep = scenes.scene(name)
+    cam = camf(w / h)
+    rs = _settings(name, w, h, seed=1)
+    renderer.upload(desc)
+    renderer.resize(w, h)
+    renderer.render(cam, rs, spp)
+    gpu = renderer.download_image()
+    ref = O.orc_render(desc, cam, rs, spp)
+    frac, mr, mg = pixel_agreement(ref, gpu)
+    exact = float((gpu.view(np.uint32) == ref.view(np.uint32)).all(axis=-1).mean())
+    print(f"{name}: {100 * frac:.3f}% of pixels within 1e-3, {100 * exact:.2f}% bit-identical, means {mr:.5f} / {mg:.5f}")
+    assert frac >= PIXEL_FRACTION
+    assert abs(mr - mg) <= MEAN_REL * mr
+    st = renderer.stats()
+    assert st.samples == spp and st.paths == w * h * spp and st.queue_overflows == 0
+
+
+def test_progressive_accumulation_matches_oracle_calls(renderer):
+    # Two render calls of 8 samples: the second starts at sample index 8, and the accumulation adds
+    # each call's per-pixel sum (CpuRenderer::render, cpu_renderer.cpp:28-32).
+    desc, camf, keep = scenes.scene("cornell")
+    w, h = 64, 48
+    cam = camf(w / h)
+    rs = _settings("cornell", w, h)
+    renderer.upload(desc)
+    renderer.resize(w, h)
+    renderer.render(cam, rs, 8)
+    renderer.render(cam, rs, 8)
+    gpu = renderer.download_image()
+    s = O.orc_render_sum(desc, cam, rs, 8, frame0=0)
+    s += O.orc_render_sum(desc, cam, rs, 8, frame0=8)
+    ref = s * np.float32(1.0 / 16)
+    frac, mr, mg = pixel_agreement(ref, gpu)
+    assert frac >= PIXEL_FRACTION and abs(mr - mg) <= MEAN_REL * mr
+    assert renderer.samples == 16
+
+
+def test_rendering_is_deterministic(renderer):
+    desc, camf, keep = scenes.scene("glass")
+    cam = camf(40 / 24)
+    renderer.upload(desc)
+    renderer.resize(40, 24)
+    imgs = []
+    for seed in (5, 5, 6):
+        renderer.reset()
+        renderer.render(cam, _settings("glass", 40, 24, seed=seed), 4)
+        imgs.append(renderer.download_image())
+    assert np.array_equal(imgs[0], imgs[1])
+    assert not np.array_equal(imgs[0], imgs[2])
+
+
+def test_furnace_and_display(renderer):
+    # test_gpu.cpp:72-103: the flat-shaded white furnace converges to 1 (< 2e-3), samples and reset
+    # behave, a linear white image displays as 0xFFFFFFFF, every display mode runs.
+    desc, camf, keep = scenes.photon_builtin("furnace", flat_normals=True)
+    renderer.upload(desc)
+    renderer.resize(64, 64)
+    rs = abi.render_settings(64, 64, max_depth=64, rr_depth=64, nee=0)
+    cam = camf(1.0)
+    renderer.render(cam, rs, 32)
+    img = renderer.download_image()
+    lum = img @ np.array([0.2126, 0.7152, 0.0722], np.float32)
+    assert np.abs(lum - 1).max() < 2e-3
+    assert renderer.samples == 32
+    renderer.reset()
+    assert renderer.samples == 0
+    rs.tonemap = abi.PT_TONEMAP_LINEAR
+    renderer.render(cam, rs, 4)
+    renderer.display(rs, abi.PT_DISPLAY_COLOR)
+    px = renderer.download_display()
+    assert px[32, 32] == 0xFFFFFFFF
+    for m in range(1, 6):
+        renderer.display(rs, m)
+    assert renderer.download_display().shape == (64, 64)
+
+
+def test_gbuffer_matches_oracle_primary_info(renderer):
+    desc, camf, keep = scenes.scene("materials")
+    w, h = 64, 36
+    cam = camf(w / h)
+    rs = _settings("materials", w, h)
+    renderer.upload(desc)
+    renderer.resize(w, h)
+    renderer.render(cam, rs, 2)
+    albedo, nd = renderer.download_gbuffer()
+    g = O.orc_gbuffer(desc, cam, rs, frame=0)
+    assert np.array_equal(albedo.view(np.uint32), g["albedo"].view(np.uint32))
+    assert np.array_equal(nd.view(np.uint32), g["normal_depth"].view(np.uint32))
+
+
+def test_upload_rejects_inconsistent_scenes(renderer):
+    desc, camf, keep = scenes.scene("box")
+    bad = abi.SceneDesc.from_buffer_copy(desc)
+    bad.num_vertices = 1  # indices now point past the vertex arrays
+    with pytest.raises(native.PhotonError) as e:
+        renderer.upload(bad)
+    assert e.value.code == abi.PT_ERR_INVALID
+
+
+def test_render_before_upload_is_an_error():
+    r = native.Renderer()
+    r.resize(8, 8)
+    with pytest.raises(native.PhotonError) as e:
+        r.render(abi.Camera(), abi.render_settings(8, 8), 1)
+    assert e.value.code == abi.PT_ERR_NO_SCENE
+    r.close()
