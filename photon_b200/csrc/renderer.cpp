@@ -63,7 +63,8 @@ void WavefrontEngine::collect_kernel_times(int iterations) {
     for (int k = 0; k < iterations; k++)
         for (int j = 0; j < 5; j++) {
             float ms = 0;
-            if (cudaEventElapsedTime(&ms, prof_ev_[size_t(6 * k + j)], prof_ev_[size_t(6 * k + j + 1)]) == cudaSuccess) kernel_ms[j] += ms;
+            PTW_CUDA(cudaEventElapsedTime(&ms, prof_ev_[size_t(6 * k + j)], prof_ev_[size_t(6 * k + j + 1)]));
+            kernel_ms[j] += ms;
         }
 }
 
@@ -127,9 +128,14 @@ void WavefrontEngine::capture(const WfParams& p) {
     cudaGraph_t g = nullptr;
     bool timed = (profile_flags_ & PT_PROFILE_KERNEL_TIMES) && int(prof_ev_.size()) >= 6 * iters;
     PTW_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < iters; k++) wf_iteration(p, shape_, stream_, timed ? &prof_ev_[size_t(6 * k)] : nullptr);
-    cudaMemcpyAsync(h_ctr_, ctr_.ptr, sizeof(Counters), cudaMemcpyDeviceToHost, stream_);
+    cudaError_t inner = cudaSuccess;
+    for (int k = 0; k < iters && inner == cudaSuccess; k++) inner = wf_iteration(p, shape_, stream_, timed ? &prof_ev_[size_t(6 * k)] : nullptr);
+    if (inner == cudaSuccess) inner = cudaMemcpyAsync(h_ctr_, ctr_.ptr, sizeof(Counters), cudaMemcpyDeviceToHost, stream_);
     cudaError_t e = cudaStreamEndCapture(stream_, &g);
+    if (inner != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        throw Error{PT_ERR_CUDA, std::string("graph capture: a captured launch failed: ") + cudaGetErrorString(inner)};
+    }
     if (e != cudaSuccess) {
         if (g) cudaGraphDestroy(g);
         throw Error{PT_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(e)};
@@ -147,6 +153,8 @@ void WavefrontEngine::capture(const WfParams& p) {
 void WavefrontEngine::run(const DevScene* scenes, int single_scene, const DevView* views, int n_views, uint64_t total_work,
                           bool count_work) {
     if (total_work == 0) return;
+    cudaError_t stale = cudaGetLastError();
+    if (stale != cudaSuccess) throw Error{PT_ERR_CUDA, std::string("an earlier CUDA call failed: ") + cudaGetErrorString(stale)};
     reserve_paths(total_work);
     ensure_shape();
     std::memset(h_ctr_, 0, sizeof(Counters));
@@ -361,6 +369,8 @@ void Renderer::render_pass_set(std::vector<DevView>& views, int /*spp_total*/, s
         profile_.shadow_node_visits += last_ctr_.shadow_node_visits;
         profile_.shadow_tri_tests += last_ctr_.shadow_tri_tests;
         bool timed = engine_->profiling() & PT_PROFILE_KERNEL_TIMES;
+        cudaError_t stale = cudaGetLastError();
+        if (stale != cudaSuccess) throw Error{PT_ERR_CUDA, std::string("after the wavefront pass: ") + cudaGetErrorString(stale)};
         if (timed) PTW_CUDA(cudaEventRecord(acc_ev_[0], stream_));
         for (size_t k = 0; k < table.size(); k++) {
             const Unit& u = pass[k];
@@ -402,7 +412,7 @@ void Renderer::render(const pt_camera& cam, const pt_render_settings& rs, int sp
     render_pass_set(views, spp, spps, f0);
     PTW_CUDA(cudaEventRecord(ev1_, stream_));
     PTW_CUDA(cudaEventSynchronize(ev1_));
-    cudaEventElapsedTime(&last_ms_, ev0_, ev1_);
+    PTW_CUDA(cudaEventElapsedTime(&last_ms_, ev0_, ev1_));
     samples_ += spp;
     last_camera_ = cam;
     heat_valid_ = false;

@@ -591,27 +591,27 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
 
 cudaError_t wf_iteration(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, cudaEvent_t* ev) {
     size_t smem = size_t(kSmemStack) * ls.trace_block * sizeof(int);
-    if (ev) cudaEventRecord(ev[0], stream);
+    if (ev) cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
     k_setup<<<1, 32, 0, stream>>>(p.ctr, p.pb.capacity);
-    if (ev) cudaEventRecord(ev[1], stream);
+    if (ev) cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal);
     k_generate<<<ls.gen_grid, ls.gen_block, 0, stream>>>(p);
-    if (ev) cudaEventRecord(ev[2], stream);
+    if (ev) cudaEventRecordWithFlags(ev[2], stream, cudaEventRecordExternal);
     if (p.count_work) k_trace<true><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
     else k_trace<false><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
-    if (ev) cudaEventRecord(ev[3], stream);
+    if (ev) cudaEventRecordWithFlags(ev[3], stream, cudaEventRecordExternal);
     k_shade<<<ls.shade_grid, ls.shade_block, 0, stream>>>(p);
-    if (ev) cudaEventRecord(ev[4], stream);
+    if (ev) cudaEventRecordWithFlags(ev[4], stream, cudaEventRecordExternal);
     if (p.count_work) k_shadow<true><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
     else k_shadow<false><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
-    if (ev) cudaEventRecord(ev[5], stream);
+    if (ev) cudaEventRecordWithFlags(ev[5], stream, cudaEventRecordExternal);
     return cudaGetLastError();
 }
 
 cudaError_t wf_accumulate(const DevView* d_view, const DevView& h_view, int first_pass, int last_pass, cudaStream_t stream) {
     uint32_t npix = uint32_t(h_view.width) * uint32_t(h_view.height);
     if (npix == 0) return cudaSuccess;
-    k_accumulate<<<(npix + 255) / 256, 256, 0, stream>>>(d_view, first_pass, last_pass);
-    return cudaGetLastError();
+    void* args[] = {const_cast<DevView**>(&d_view), &first_pass, &last_pass};
+    return cudaLaunchKernel(reinterpret_cast<const void*>(&k_accumulate), dim3((npix + 255) / 256), dim3(256), args, 0, stream);
 }
 
 cudaError_t wf_trace_primary(const DevScene* scene, const float* cam16, int w, int h, uint32_t frame, uint32_t seed, float4* out,
