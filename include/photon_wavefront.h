@@ -234,8 +234,11 @@ typedef struct pt_tuning {
     int32_t path_capacity;     /* paths in flight */
     int32_t trace_block;       /* threads per block of the traversal kernels */
     int32_t shade_block;       /* threads per block of the shading kernel */
-    int32_t sort_by_material;  /* 1: shade in material order, 0: in queue order, -1: keep */
+    int32_t sort_by_material;  /* reserved (0) */
     int32_t graph_bounces;     /* bounce iterations captured per CUDA graph launch */
+    int32_t sort_rays;         /* 0 off, 1-4: sort continuing rays by direction octant + Morton origin cell
+                                  with this many bits per axis before tracing them; -1 keep */
+    int32_t packed;            /* 1: f32x2 (packed FP32) slab tests in traversal, 0: scalar; -1 keep */
 } pt_tuning;
 int32_t pt_set_tuning(pt_renderer* r, const pt_tuning* t);
 int32_t pt_get_tuning(const pt_renderer* r, pt_tuning* t);

@@ -189,6 +189,24 @@ void DeviceScene::upload(const pt_scene_desc& d, cudaStream_t s, bool lights_onl
     v.p_punctual = d.p_punctual;
     v.has_lights = (d.p_env + d.p_emissive + d.p_punctual) > 0 ? 1 : 0;
     v.bvh_depth = 0;
+    {
+        float lo[3] = {d.bounds_min.x, d.bounds_min.y, d.bounds_min.z}, hi[3] = {d.bounds_max.x, d.bounds_max.y, d.bounds_max.z};
+        float inv[3];
+        for (int k = 0; k < 3; k++) {
+            float e = hi[k] - lo[k];
+            if (!(e > 0) || !std::isfinite(e)) {
+                lo[k] = 0;
+                e = 1;
+            }
+            inv[k] = 1.0f / e;
+        }
+        v.bounds_lo_x = lo[0];
+        v.bounds_lo_y = lo[1];
+        v.bounds_lo_z = lo[2];
+        v.inv_extent_x = inv[0];
+        v.inv_extent_y = inv[1];
+        v.inv_extent_z = inv[2];
+    }
     d_view_.upload(&v, 1, s);
     PTW_CUDA(cudaStreamSynchronize(s));
     float dx = d.bounds_max.x - d.bounds_min.x, dy = d.bounds_max.y - d.bounds_min.y, dz = d.bounds_max.z - d.bounds_min.z;

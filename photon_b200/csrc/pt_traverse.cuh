@@ -54,11 +54,51 @@ PT_HD bool tri_intersect(float4 g0, float4 g1, float4 g2, V3 o, V3 d, float tmax
     return t > 0.0f && t < tmax;
 }
 
-// One traversal. `stack` points at this thread's column of the block's shared stack (entry k at
-// stack[k * stride]). AnyHit stops at the first accepted triangle. Returns whether a hit was found.
-template <bool AnyHit, bool Count>
+// Packed FP32 pairs (sm_100 add/sub/mul.rn.f32x2): two IEEE round-to-nearest operations per
+// instruction, each rounded exactly as the scalar operation, so results are bit-identical. A float4
+// loaded by one 128-bit load sits in a register quad, so its (x, y) and (z, w) halves are pairs.
+typedef unsigned long long f32x2;
+PT_HD f32x2 pack2(float a, float b) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+PT_HD void unpack2(f32x2 r, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r)); }
+PT_HD f32x2 sub2(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+PT_HD f32x2 mul2(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
+// The slab test of box_entry with the (bmin - o) * inv_d products computed in pairs; the min/max
+// reduction is unchanged (there is no packed min/max).
+struct RayPairs {
+    f32x2 oxy, oz0, ixy, iz0;
+};
+PT_HD RayPairs ray_pairs(V3 o, V3 inv_d) { return {pack2(o.x, o.y), pack2(o.z, 0.0f), pack2(inv_d.x, inv_d.y), pack2(inv_d.z, 0.0f)}; }
+PT_HD float box_entry2(float4 bmin, float4 bmax, const RayPairs& r, float tmax) {
+    float tx0, ty0, tz0, tx1, ty1, tz1, w0, w1;
+    unpack2(mul2(sub2(pack2(bmin.x, bmin.y), r.oxy), r.ixy), tx0, ty0);
+    unpack2(mul2(sub2(pack2(bmin.z, bmin.w), r.oz0), r.iz0), tz0, w0);
+    unpack2(mul2(sub2(pack2(bmax.x, bmax.y), r.oxy), r.ixy), tx1, ty1);
+    unpack2(mul2(sub2(pack2(bmax.z, bmax.w), r.oz0), r.iz0), tz1, w1);
+    float tnear = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
+    float tfar = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
+    return tnear <= tfar ? tnear : kInf;
+}
+
+// One traversal (traverse.h:66-138): nearest-first, leaves tested in place, `stack` is this thread's
+// column of the block's shared stack (entry k at stack[k * stride]). AnyHit stops at the first
+// accepted triangle. Packed selects the f32x2 slab test (bit-identical results).
+template <bool AnyHit, bool Count, bool Packed = true>
 PT_HD bool traverse(const DevScene& s, V3 o, V3 d, float tmax, Hit& hit, int* stack, int stride, TraversalCounters* cnt) {
     V3 inv_d{safe_inv(d.x), safe_inv(d.y), safe_inv(d.z)};
+    RayPairs rp = ray_pairs(o, inv_d);
     int overflow[kStackSize - kSmemStack];
     int sp = 0;
     int node = 0;
@@ -69,8 +109,8 @@ PT_HD bool traverse(const DevScene& s, V3 o, V3 d, float tmax, Hit& hit, int* st
         const float4* n = nodes + 4 * node;
         float4 n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2), n3 = __ldg(n + 3);
         if (Count) cnt->nodes++;
-        float tl = box_entry(n0, n1, o, inv_d, tmax);
-        float tr = box_entry(n2, n3, o, inv_d, tmax);
+        float tl = Packed ? box_entry2(n0, n1, rp, tmax) : box_entry(n0, n1, o, inv_d, tmax);
+        float tr = Packed ? box_entry2(n2, n3, rp, tmax) : box_entry(n2, n3, o, inv_d, tmax);
         int next0 = 0, next1 = 0;
         float tn0 = 0, tn1 = 0;
         int nn = 0;

@@ -41,6 +41,8 @@ struct DevScene {
     float p_env, p_emissive, p_punctual;
     int has_lights;
     int bvh_depth;
+    float bounds_lo_x, bounds_lo_y, bounds_lo_z;   // scene box (for ray-sort keys)
+    float inv_extent_x, inv_extent_y, inv_extent_z;
 };
 
 }  // namespace ptw

@@ -87,6 +87,7 @@ void WavefrontEngine::reserve_paths(uint64_t needed) {
     pb_.sh0 = bufs_[9].ptr;
     pb_.sh1 = bufs_[10].ptr;
     pb_.sh2 = bufs_[11].ptr;
+    keys_.allocate(want);
     pb_.capacity = uint32_t(want);
     if (graph_) {
         cudaGraphExecDestroy(graph_);
@@ -102,6 +103,13 @@ size_t WavefrontEngine::device_bytes() const {
 }
 
 void WavefrontEngine::ensure_shape() {
+    if (tuning_.sort_rays > 0 && hist_.count < (size_t(8) << (3 * tuning_.sort_rays))) {
+        size_t buckets = size_t(8) << (3 * tuning_.sort_rays);
+        hist_.allocate(buckets);
+        offsets_.allocate(buckets);
+        hist_.zero(stream_);
+        PTW_CUDA(cudaStreamSynchronize(stream_));
+    }
     if (shape_ok_) return;
     PTW_CUDA(wf_launch_shape(device_, tuning_.trace_block, tuning_.shade_block, &shape_));
     shape_ok_ = true;
@@ -116,6 +124,11 @@ WfParams WavefrontEngine::params(const DevScene* scenes, int single, const DevVi
     p.pb = pb_;
     p.ctr = ctr_.ptr;
     p.count_work = count ? 1 : 0;
+    p.packed = tuning_.packed ? 1 : 0;
+    p.sort_bits = tuning_.sort_rays;
+    p.keys = keys_.ptr;
+    p.hist = hist_.ptr;
+    p.offsets = offsets_.ptr;
     return p;
 }
 
@@ -566,6 +579,11 @@ void Renderer::set_tuning(const pt_tuning& t) {
     }
     if (t.sort_by_material >= 0) cur.sort_by_material = t.sort_by_material;
     if (t.graph_bounces >= 0) cur.graph_bounces = t.graph_bounces;
+    if (t.sort_rays >= 0) {
+        if (t.sort_rays > 4) throw Error{PT_ERR_INVALID, "sort_rays must be in [0, 4]"};
+        cur.sort_rays = t.sort_rays;
+    }
+    if (t.packed >= 0) cur.packed = t.packed ? 1 : 0;
     engine_->set_tuning(cur);
 }
 
@@ -576,6 +594,9 @@ void Renderer::get_tuning(pt_tuning* t) const {
     t->shade_block = c.shade_block;
     t->sort_by_material = c.sort_by_material;
     t->graph_bounces = c.graph_bounces;
+    t->sort_rays = c.sort_rays;
+    t->packed = c.packed;
+    t->sort_by_material = 0;
 }
 
 void Renderer::trace_primary(const pt_camera& cam, int w, int h, uint32_t frame, uint32_t seed, float* hits4) {

@@ -21,6 +21,8 @@ struct Tuning {
     int shade_block = 128;
     int sort_by_material = 0;
     int graph_bounces = 4;         // iterations per CUDA graph launch
+    int sort_rays = 0;             // origin bits per axis of the ray-sort key (0: no sorting)
+    int packed = 1;                // f32x2 slab tests
 };
 
 // Runs wavefront passes over a table of views on one device stream. Owns the path pool, the
@@ -79,6 +81,7 @@ private:
     DeviceBuffer<float4> bufs_[12];
     DeviceBuffer<uint4> ids_[2];
     DeviceBuffer<Counters> ctr_;
+    DeviceBuffer<uint32_t> keys_, hist_, offsets_;
     Counters* h_ctr_ = nullptr;
     Counters last_{};
     cudaGraphExec_t graph_ = nullptr;

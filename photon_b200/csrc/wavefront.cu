@@ -127,7 +127,7 @@ __global__ void k_setup(Counters* c, uint32_t capacity) {
     c->shadow_rays += c->shadow_count;
     c->shadow_count = 0;
     c->rays += cnt + n;
-    c->fetch[0] = c->fetch[1] = c->fetch[2] = c->fetch[3] = 0;
+    for (int k = 0; k < 6; k++) c->fetch[k] = 0;
     if (cnt + n > 0) c->iterations++;
 }
 
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(256) k_generate(const __grid_constant__ WfPara
 }
 
 // ---- trace: closest hit (traverse.h:140-142) -------------------------------------------------------
-template <bool Count>
+template <bool Count, bool Packed>
 __global__ void __launch_bounds__(256) k_trace(const __grid_constant__ WfParams P) {
     extern __shared__ int smem_stack[];
     int* stack = smem_stack + threadIdx.x;
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(256) k_trace(const __grid_constant__ WfParams 
             int view = P.single_scene >= 0 ? 0 : int(P.pb.id[p][i].x);
             const DevScene& s = scene_for(P, view);
             Hit h{kInf, -1, 0.0f, 0.0f};
-            traverse<false, Count>(s, xyz(o4), xyz(d4), kInf, h, stack, blockDim.x, &tc);
+            traverse<false, Count, Packed>(s, xyz(o4), xyz(d4), kInf, h, stack, blockDim.x, &tc);
             P.pb.hit[i] = make_float4(h.t, __int_as_float(h.tri), h.u, h.v);
         }
     }
@@ -189,6 +189,30 @@ __global__ void __launch_bounds__(256) k_trace(const __grid_constant__ WfParams 
         warp_add_u64(&c->node_visits, tc.nodes);
         warp_add_u64(&c->tri_tests, tc.tris);
     }
+}
+
+// Sort key of a continuing ray: direction octant, then the Morton code of its origin's cell in the
+// scene box (`bits` per axis). Rays in one bucket start close together and head the same way, so
+// a warp of them walks similar nodes.
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+    v &= 0x3ff;
+    v = (v | (v << 16)) & 0x030000FF;
+    v = (v | (v << 8)) & 0x0300F00F;
+    v = (v | (v << 4)) & 0x030C30C3;
+    v = (v | (v << 2)) & 0x09249249;
+    return v;
+}
+__device__ __forceinline__ uint32_t ray_key(const DevScene& s, V3 o, V3 d, int bits) {
+    float cells = float(1u << bits);
+    auto cell = [&](float x, float lo, float inv) {
+        float f = (x - lo) * inv * cells;
+        f = fminf(fmaxf(f, 0.0f), cells - 1.0f);
+        return uint32_t(f);
+    };
+    uint32_t m = spread3(cell(o.x, s.bounds_lo_x, s.inv_extent_x)) | (spread3(cell(o.y, s.bounds_lo_y, s.inv_extent_y)) << 1) |
+                 (spread3(cell(o.z, s.bounds_lo_z, s.inv_extent_z)) << 2);
+    uint32_t oct = (d.x < 0 ? 1u : 0u) | (d.y < 0 ? 2u : 0u) | (d.z < 0 ? 4u : 0u);
+    return (oct << (3 * bits)) | m;
 }
 
 // ---- shade: one vertex of trace_path (integrator.h:158-262) -----------------------------------------
@@ -307,6 +331,14 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ WfParams 
         }
         // Continuing paths move to the other buffer, compacted.
         uint32_t slot = warp_append(cont, &c->count[q]);
+        if (P.sort_bits > 0) {
+            uint32_t key = cont ? ray_key(scene_for(P, id.x), ro, rd, P.sort_bits) : 0xffffffffu;
+            uint32_t peers = __match_any_sync(kFull, key);
+            if (cont) {
+                P.keys[slot] = key;
+                if (int(lane_id()) == __ffs(peers) - 1) atomicAdd(&P.hist[key], uint32_t(__popc(peers)));
+            }
+        }
         if (cont) {
             P.pb.o[q][slot] = make_float4(ro.x, ro.y, ro.z, prev_pdf);
             P.pb.d[q][slot] = make_float4(rd.x, rd.y, rd.z, __uint_as_float(flags));
@@ -338,7 +370,7 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ WfParams 
 }
 
 // ---- shadow: any hit (traverse.h:144-147) --------------------------------------------------------------
-template <bool Count>
+template <bool Count, bool Packed>
 __global__ void __launch_bounds__(256) k_shadow(const __grid_constant__ WfParams P) {
     extern __shared__ int smem_stack[];
     int* stack = smem_stack + threadIdx.x;
@@ -355,7 +387,7 @@ __global__ void __launch_bounds__(256) k_shadow(const __grid_constant__ WfParams
         uint32_t view = tag & 0x7fffffffu;
         const DevScene& s = scene_for(P, int(view));
         Hit h{kInf, -1, 0.0f, 0.0f};
-        bool occ = traverse<true, Count>(s, xyz(a), xyz(b), a.w, h, stack, blockDim.x, &tc);
+        bool occ = traverse<true, Count, Packed>(s, xyz(a), xyz(b), a.w, h, stack, blockDim.x, &tc);
         if (!occ) {
             uint32_t target = __float_as_uint(b.w);
             if (tag & 0x80000000u) {
@@ -376,6 +408,66 @@ __global__ void __launch_bounds__(256) k_shadow(const __grid_constant__ WfParams
         warp_add_u64(&c->shadow_node_visits, tc.nodes);
         warp_add_u64(&c->shadow_tri_tests, tc.tris);
     }
+}
+
+// ---- ray sorting: a counting sort of the shade output by ray key ------------------------------------------
+// Exclusive scan of the bucket counts into write offsets (one block), then zero the counts.
+__global__ void __launch_bounds__(1024) k_sort_scan(const __grid_constant__ WfParams P, uint32_t buckets) {
+    __shared__ uint32_t part[1024];
+    uint32_t per = (buckets + 1023) / 1024;
+    uint32_t lo = threadIdx.x * per, hi = min(lo + per, buckets);
+    uint32_t sum = 0;
+    for (uint32_t k = lo; k < hi; k++) sum += P.hist[k];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024; off <<= 1) {
+        uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t run = part[threadIdx.x] - sum;  // exclusive prefix of this thread's range
+    for (uint32_t k = lo; k < hi; k++) {
+        uint32_t h = P.hist[k];
+        P.offsets[k] = run;
+        run += h;
+        P.hist[k] = 0;
+    }
+}
+
+// Moves every continuing path from the shade output into the (now free) input buffer at its
+// bucket's next position; the next setup then finds the sorted paths there.
+__global__ void __launch_bounds__(256) k_sort_scatter(const __grid_constant__ WfParams P) {
+    Counters* c = P.ctr;
+    const uint32_t p = c->parity, q = p ^ 1u, n = c->count[q];
+    for (;;) {
+        uint32_t i0 = warp_fetch(&c->fetch[4]);
+        if (i0 >= n) break;
+        uint32_t i = i0 + lane_id();
+        uint32_t key = i < n ? P.keys[i] : 0xffffffffu;
+        uint32_t peers = __match_any_sync(kFull, key);
+        int leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (i < n && int(lane_id()) == leader) base = atomicAdd(&P.offsets[key], uint32_t(__popc(peers)));
+        base = __shfl_sync(kFull, base, leader);
+        if (i < n) {
+            uint32_t dst = base + __popc(peers & ((1u << lane_id()) - 1u));
+            P.pb.o[p][dst] = P.pb.o[q][i];
+            P.pb.d[p][dst] = P.pb.d[q][i];
+            P.pb.beta[p][dst] = P.pb.beta[q][i];
+            P.pb.lr[p][dst] = P.pb.lr[q][i];
+            P.pb.id[p][dst] = P.pb.id[q][i];
+        }
+    }
+}
+
+// After the scatter: the sorted paths live in the input buffer; make the next setup flip to it.
+__global__ void k_sort_finish(Counters* c) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t p = c->parity, q = p ^ 1u;
+    c->count[p] = c->count[q];
+    c->count[q] = 0;
+    c->parity = q;
 }
 
 // ---- accumulate: CpuRenderer's per-pixel sum in sample order (cpu_renderer.cpp:28-31) ------------------
@@ -566,19 +658,18 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
     out->gen_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
     out->trace_block = trace_block;
     size_t smem = size_t(kSmemStack) * trace_block * sizeof(int);
-    e = cudaFuncSetAttribute(k_trace<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_trace<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_shadow<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_shadow<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace<false>, trace_block, smem);
+    const void* smem_kernels[] = {(const void*)k_trace<false, false>, (const void*)k_trace<false, true>, (const void*)k_trace<true, false>,
+                                  (const void*)k_trace<true, true>,   (const void*)k_shadow<false, false>, (const void*)k_shadow<false, true>,
+                                  (const void*)k_shadow<true, false>, (const void*)k_shadow<true, true>};
+    for (const void* k : smem_kernels) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return e;
+    }
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace<false, true>, trace_block, smem);
     if (e != cudaSuccess) return e;
     out->trace_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
     out->shadow_block = trace_block;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shadow<false>, trace_block, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shadow<false, true>, trace_block, smem);
     if (e != cudaSuccess) return e;
     out->shadow_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
     out->shade_block = shade_block;
@@ -589,6 +680,22 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
     return cudaSuccess;
 }
 
+template <bool Count, bool Packed>
+static void launch_traversals(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, size_t smem, bool shadow) {
+    if (shadow) k_shadow<Count, Packed><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
+    else k_trace<Count, Packed><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
+}
+
+static void launch_traversal(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, size_t smem, bool shadow) {
+    if (p.count_work) {
+        if (p.packed) launch_traversals<true, true>(p, ls, stream, smem, shadow);
+        else launch_traversals<true, false>(p, ls, stream, smem, shadow);
+    } else {
+        if (p.packed) launch_traversals<false, true>(p, ls, stream, smem, shadow);
+        else launch_traversals<false, false>(p, ls, stream, smem, shadow);
+    }
+}
+
 cudaError_t wf_iteration(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, cudaEvent_t* ev) {
     size_t smem = size_t(kSmemStack) * ls.trace_block * sizeof(int);
     if (ev) cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
@@ -596,13 +703,16 @@ cudaError_t wf_iteration(const WfParams& p, const LaunchShape& ls, cudaStream_t 
     if (ev) cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal);
     k_generate<<<ls.gen_grid, ls.gen_block, 0, stream>>>(p);
     if (ev) cudaEventRecordWithFlags(ev[2], stream, cudaEventRecordExternal);
-    if (p.count_work) k_trace<true><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
-    else k_trace<false><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
+    launch_traversal(p, ls, stream, smem, false);
     if (ev) cudaEventRecordWithFlags(ev[3], stream, cudaEventRecordExternal);
     k_shade<<<ls.shade_grid, ls.shade_block, 0, stream>>>(p);
     if (ev) cudaEventRecordWithFlags(ev[4], stream, cudaEventRecordExternal);
-    if (p.count_work) k_shadow<true><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
-    else k_shadow<false><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
+    launch_traversal(p, ls, stream, smem, true);
+    if (p.sort_bits > 0) {
+        k_sort_scan<<<1, 1024, 0, stream>>>(p, 8u << (3 * p.sort_bits));
+        k_sort_scatter<<<ls.gen_grid, ls.gen_block, 0, stream>>>(p);
+        k_sort_finish<<<1, 32, 0, stream>>>(p.ctr);
+    }
     if (ev) cudaEventRecordWithFlags(ev[5], stream, cudaEventRecordExternal);
     return cudaGetLastError();
 }

@@ -35,11 +35,12 @@ struct DevView {
 // Device counters of one wavefront run. The kernels read the iteration's sizes from here, so a
 // bounce iteration is a fixed launch sequence that a CUDA graph can replay.
 struct Counters {
-    uint32_t parity;                 // buffer holding this iteration's paths
+    uint32_t parity;                 // buffer holding this iteration's paths (the sort step sets it so
+                                     // that the next setup finds the sorted paths)
     uint32_t count[2];               // paths in each buffer
     uint32_t shadow_count;
     uint32_t gen_base, gen_n;        // slots filled by this iteration's generate step
-    uint32_t fetch[4];               // work-claim counters of generate / trace / shade / shadow
+    uint32_t fetch[6];               // work-claim counters: generate, trace, shade, shadow, sort scatter
     uint32_t overflow;
     uint32_t iterations;
     unsigned long long work_base, work_next, work_total;
@@ -69,6 +70,12 @@ struct WfParams {
     PathBuffers pb;
     Counters* ctr;
     int count_work;            // 1: count node visits / triangle tests (stats runs)
+    int packed;                // 1: f32x2 slab tests in the traversal kernels
+    int sort_bits;             // > 0: sort continuing paths by direction octant + Morton origin cell
+                               //      (this many bits per axis) before they are traced
+    uint32_t* keys;            // capacity entries (sort keys of the shade output)
+    uint32_t* hist;            // 8 << (3 * sort_bits) bucket counts (zero between iterations)
+    uint32_t* offsets;         // bucket write positions of the scatter
 };
 
 // A camera passed by value to the probe kernels (pt_camera as 16 floats).
