@@ -184,6 +184,53 @@ def run_reference(args, world, rank):
     return 0
 
 
+def systems_sections(r, g, desc, rank):
+    """The batched and served forms on the same 262K scene (extra keys of the JSON line):
+    - batched: 64 seeded views (320x180..1920x1080, spp {1,4,16,64}, cameras on a sphere of radius
+      1.5x the scene extent) in one pt_render_views call, against the same views rendered one
+      pt_render call at a time;
+    - served: a Poisson stream of 200 requests at 20 req/s over the 36-triangle box and the 262K scene
+      (resolution / spp / depth drawn as in the serving configuration) through the server, against
+      the same stream rendered one request at a time in arrival order; p50/p99 latency from
+      submission to result."""
+    from photon_b200 import abi, native, serving, workloads
+    out = {}
+    views = workloads.batch_views(desc, 64, seed=2)
+    total = sum(v.width * v.height * v.spp for v in views)
+    r.render_views(views)
+    t0 = time.perf_counter()
+    r.render_views(views)
+    tb = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for v in views:
+        r.resize(v.width, v.height)
+        r.reset()
+        r.render(v.camera, abi.RenderSettings(v.width, v.height, v.path, 1.0, abi.PT_TONEMAP_ACES, v.seed), v.spp)
+    tp = time.perf_counter() - t0
+    out["batched"] = {"workload": "64 views of the 262K scene (seed 2)", "samples": total, "msamples_per_s": total / tb / 1e6,
+                      "plain_msamples_per_s": total / tp / 1e6, "batched_over_plain": tp / tb, "api": "pt_render_views"}
+    gb = native.box_scene()
+    bb = gb.build()
+    server = native.Server(budget_bytes=150 << 30)
+    sid_b = server.add_scene(bb.desc)
+    sid_t = server.add_scene(desc)
+    stream = workloads.request_stream([(sid_b, bb.desc), (sid_t, desc)], 200, 20.0, seed=7)
+    served = serving.run_served(server, stream)
+    server.close()
+    rb = native.Renderer(r_device(r))
+    rb.upload(bb.desc)
+    plain = serving.run_plain({sid_b: rb, sid_t: r}, stream)
+    rb.close()
+    out["served"] = {"workload": "Poisson, 200 requests at 20 req/s, seed 7, scenes: 36-triangle box + 262K terrain",
+                     "served": served, "plain": plain, "budget_bytes": 150 << 30}
+    return out
+
+
+def r_device(r):
+    import torch
+    return torch.cuda.current_device()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -191,6 +238,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-systems", action="store_true", help="skip the batched-views and served-stream sections")
     args = ap.parse_args()
     world, rank, local = dist_info()
     if args.impl == "reference":
@@ -298,6 +346,8 @@ def main():
             "kernel_share": {k: v / ktotal for k, v in kernels.items()},
             "roofline": roofline,
             "clocks": clock_info}
+    if not args.no_systems:
+        line.update(systems_sections(r, g, desc, rank))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(desc, cam)
     if rank == 0:

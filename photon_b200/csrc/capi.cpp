@@ -199,6 +199,12 @@ int32_t pt_set_tuning(pt_renderer* r, const pt_tuning* t) {
     PT_RENDERER_CALL(r, r->r->set_tuning(*t));
 }
 
+int32_t pt_autotune(pt_renderer* r, const pt_camera* camera, const pt_render_settings* settings, int32_t spp, uint64_t probe_samples,
+                    pt_tuning* chosen, double* default_rate, double* tuned_rate) {
+    if (!camera || !settings) return PT_ERR_INVALID;
+    PT_RENDERER_CALL(r, r->r->autotune(*camera, *settings, spp, probe_samples, chosen, default_rate, tuned_rate));
+}
+
 int32_t pt_get_tuning(const pt_renderer* r, pt_tuning* t) {
     if (!r || !r->r || !t) return PT_ERR_INVALID;
     r->r->get_tuning(t);

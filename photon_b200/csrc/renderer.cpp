@@ -599,6 +599,65 @@ void Renderer::get_tuning(pt_tuning* t) const {
     t->sort_by_material = 0;
 }
 
+// Coordinate descent over the knobs, one at a time, each candidate timed on the same probe (a view
+// of the camera at a reduced resolution so that it holds about probe_samples paths). Every probe
+// runs twice and keeps the faster time, after a warm-up render with the candidate (graph capture and
+// buffer growth are not timed).
+void Renderer::autotune(const pt_camera& cam, const pt_render_settings& rs, int spp, uint64_t probe_samples, pt_tuning* chosen,
+                        double* default_rate, double* tuned_rate) {
+    if (!scene_.ready()) throw Error{PT_ERR_NO_SCENE, "autotune before upload"};
+    if (spp <= 0 || rs.width <= 0 || rs.height <= 0) throw Error{PT_ERR_INVALID, "autotune: bad view"};
+    if (probe_samples == 0) probe_samples = uint64_t(1) << 23;
+    double full = double(rs.width) * double(rs.height) * double(spp);
+    double scale = std::min(1.0, std::sqrt(double(probe_samples) / full));
+    pt_view v{};
+    v.camera = cam;
+    v.width = std::max(8, int(rs.width * scale));
+    v.height = std::max(8, int(rs.height * scale));
+    v.spp = spp;
+    v.seed = rs.seed;
+    v.path = rs.path;
+    uint64_t samples = uint64_t(v.width) * uint64_t(v.height) * uint64_t(spp);
+    std::vector<pt_view> saved_views = batch_views_;
+    auto time_probe = [&]() {
+        render_views(&v, 1);  // warm-up (graph capture, buffer growth)
+        float best = 1e30f;
+        for (int k = 0; k < 2; k++) {
+            render_views(&v, 1);
+            best = std::min(best, last_ms_);
+        }
+        return double(samples) / (double(best) / 1000.0);
+    };
+    Tuning base = engine_->tuning();
+    engine_->set_tuning(base);
+    double best_rate = time_probe();
+    if (default_rate) *default_rate = best_rate;
+    Tuning best = base;
+    auto try_knob = [&](auto setter, std::initializer_list<int> values) {
+        Tuning start = best;
+        for (int val : values) {
+            Tuning t = start;
+            setter(t, val);
+            engine_->set_tuning(t);
+            double rate = time_probe();
+            if (rate > best_rate * 1.01) {
+                best_rate = rate;
+                best = t;
+            }
+        }
+        engine_->set_tuning(best);
+    };
+    try_knob([](Tuning& t, int v) { t.path_capacity = v; }, {1 << 19, 1 << 20, 1 << 21, 1 << 22});
+    try_knob([](Tuning& t, int v) { t.trace_block = v; }, {64, 128, 256});
+    try_knob([](Tuning& t, int v) { t.shade_block = v; }, {64, 128, 256});
+    try_knob([](Tuning& t, int v) { t.graph_bounces = v; }, {2, 4, 8});
+    try_knob([](Tuning& t, int v) { t.sort_rays = v; }, {0, 3});
+    engine_->set_tuning(best);
+    batch_views_ = saved_views;
+    if (tuned_rate) *tuned_rate = best_rate;
+    if (chosen) get_tuning(chosen);
+}
+
 void Renderer::trace_primary(const pt_camera& cam, int w, int h, uint32_t frame, uint32_t seed, float* hits4) {
     if (!scene_.ready()) throw Error{PT_ERR_NO_SCENE, "trace before upload"};
     if (w <= 0 || h <= 0) return;
@@ -661,11 +720,25 @@ void Renderer::render_views(const pt_view* views, int n) {
         }
         spps[size_t(i)] = pv.spp;
     }
+    // One pass when it fits: the radiance buffer may take up to half of the free device memory.
+    uint64_t total = 0;
+    for (int i = 0; i < n; i++) total += uint64_t(views[i].width) * uint64_t(views[i].height) * uint64_t(views[i].spp);
+    size_t free_b = 0, total_b = 0;
+    PTW_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    uint64_t saved_cap = sample_cap_;
+    uint64_t room = uint64_t(free_b / 2) / sizeof(float4) + sample_out_.count;
+    sample_cap_ = std::max<uint64_t>(saved_cap, std::min<uint64_t>(total, room));
     PTW_CUDA(cudaEventRecord(ev0_, stream_));
-    render_pass_set(table, 0, spps, f0);
+    try {
+        render_pass_set(table, 0, spps, f0);
+    } catch (...) {
+        sample_cap_ = saved_cap;
+        throw;
+    }
+    sample_cap_ = saved_cap;
     PTW_CUDA(cudaEventRecord(ev1_, stream_));
     PTW_CUDA(cudaEventSynchronize(ev1_));
-    cudaEventElapsedTime(&last_ms_, ev0_, ev1_);
+    PTW_CUDA(cudaEventElapsedTime(&last_ms_, ev0_, ev1_));
 }
 
 void Renderer::download_view(int v, float* rgb, size_t n) {

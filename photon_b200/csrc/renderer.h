@@ -114,6 +114,8 @@ public:
     void stats(pt_stats* out) const;
     void set_tuning(const pt_tuning& t);
     void get_tuning(pt_tuning* t) const;
+    void autotune(const pt_camera& cam, const pt_render_settings& rs, int spp, uint64_t probe_samples, pt_tuning* chosen,
+                  double* default_rate, double* tuned_rate);
 
     void trace_primary(const pt_camera& cam, int w, int h, uint32_t frame, uint32_t seed, float* hits4);
     void light_picks(const pt_camera& cam, const pt_render_settings& rs, uint32_t frame, int32_t* picks4);

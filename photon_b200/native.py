@@ -56,6 +56,8 @@ def _load():
         "pt_get_profile": ([C.c_void_p, P(abi.Profile)], C.c_int32),
         "pt_set_tuning": ([C.c_void_p, P(abi.Tuning)], C.c_int32),
         "pt_get_tuning": ([C.c_void_p, P(abi.Tuning)], C.c_int32),
+        "pt_autotune": ([C.c_void_p, P(abi.Camera), P(abi.RenderSettings), C.c_int32, C.c_uint64, P(abi.Tuning),
+                         P(C.c_double), P(C.c_double)], C.c_int32),
         "pt_trace_primary": ([C.c_void_p, P(abi.Camera), C.c_int32, C.c_int32, C.c_uint32, C.c_uint32, _f32p], C.c_int32),
         "pt_light_picks_primary": ([C.c_void_p, P(abi.Camera), P(abi.RenderSettings), C.c_uint32, _i32p], C.c_int32),
         "pt_heatmap": ([C.c_void_p, P(abi.Camera), C.c_int32, C.c_int32, _f32p], C.c_int32),
@@ -212,6 +214,13 @@ class Renderer:
         for k, v in kw.items():
             setattr(t, k, v)
         _check(lib.pt_set_tuning(self.h, C.byref(t)), self._err)
+
+    def autotune(self, cam, rs, spp, probe_samples=0):
+        """Runs the autotuner; returns (chosen tuning dict, default rate, tuned rate) in samples/s."""
+        t = abi.Tuning()
+        d, b = C.c_double(), C.c_double()
+        _check(lib.pt_autotune(self.h, C.byref(cam), C.byref(rs), spp, probe_samples, C.byref(t), C.byref(d), C.byref(b)), self._err)
+        return {n: getattr(t, n) for n, _ in abi.Tuning._fields_}, d.value, b.value
 
     def tuning(self):
         t = abi.Tuning()

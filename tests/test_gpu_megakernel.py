@@ -83,3 +83,41 @@ def test_throughput_vs_photon_megakernel(L):
     rec["speedup"] = rec["wavefront_msamples_per_s"] / rec["megakernel_msamples_per_s"]
     print("MEGAKERNEL_COMPARISON " + json.dumps(rec))
     assert rec["speedup"] > 1.0
+
+
+def test_batched_views_vs_photon_megakernel(L):
+    # The 64-view batched workload: one wavefront over every view, against Photon's megakernel
+    # rendering each view (8-spp launches, as `photon bench`).
+    from photon_b200 import workloads
+    desc, camf, keep = scenes.scene("terrain")
+    views = workloads.batch_views(desc, 64, seed=2)
+    total = sum(v.width * v.height * v.spp for v in views)
+    r = native.Renderer()
+    r.upload(desc)
+    r.render_views(views)
+    t0 = time.perf_counter()
+    r.render_views(views)
+    wf = time.perf_counter() - t0
+    r.close()
+    ref_scene = O.RefScene.from_desc(desc, lib=L)
+    g = L.refgpu_create()
+    try:
+        assert L.refgpu_upload(g, ref_scene.h)
+        L.refgpu_resize(g, 64, 64)
+        L.refgpu_render(g, C.byref(views[0].camera), C.byref(abi.render_settings(64, 64, max_depth=12)), 4)
+        t0 = time.perf_counter()
+        for v in views:
+            L.refgpu_resize(g, v.width, v.height)
+            L.refgpu_reset(g)
+            rs = abi.RenderSettings(v.width, v.height, v.path, 1.0, abi.PT_TONEMAP_ACES, v.seed)
+            done = 0
+            while done < v.spp:
+                k = min(8, v.spp - done)
+                L.refgpu_render(g, C.byref(v.camera), C.byref(rs), k)
+                done += k
+        mk = time.perf_counter() - t0
+    finally:
+        L.refgpu_destroy(g)
+    rec = {"batched_msamples_per_s": total / wf / 1e6, "megakernel_msamples_per_s": total / mk / 1e6, "speedup": mk / wf}
+    print("BATCHED_VS_MEGAKERNEL " + json.dumps(rec))
+    assert rec["speedup"] > 1.0

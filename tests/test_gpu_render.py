@@ -177,3 +177,24 @@ def test_render_before_upload_is_an_error():
         r.render(abi.Camera(), abi.render_settings(8, 8), 1)
     assert e.value.code == abi.PT_ERR_NO_SCENE
     r.close()
+
+
+@pytest.mark.parametrize("name", ["box", "terrain", "cornell"])
+def test_gpu_matches_golden_fixtures(renderer, name):
+    # The committed fixtures were produced by Photon's own CPU build (tests/golden/make_golden.py).
+    import test_golden
+    z, cam, rs, spp = test_golden.load(name)
+    if name == "cornell":
+        keep = O.RefScene.builtin("cornell")
+        desc = keep.desc
+    else:
+        keep = (native.box_scene() if name == "box" else native.terrain_scene())
+        built = keep.build()
+        desc = built.desc
+    renderer.upload(desc)
+    renderer.resize(rs.width, rs.height)
+    assert np.array_equal(renderer.trace_primary(cam, rs.width, rs.height, 0, rs.seed).view(np.uint32), z["hits"].view(np.uint32))
+    assert np.array_equal(renderer.light_picks(cam, rs, 0), z["picks"])
+    renderer.render(cam, rs, spp)
+    frac, ma, mb = pixel_agreement(z["image"], renderer.download_image())
+    assert frac >= PIXEL_FRACTION and abs(ma - mb) <= MEAN_REL * ma

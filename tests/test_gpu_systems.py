@@ -1,0 +1,161 @@
+"""The systems forms beside the drop-in renderer (gpu): batched views in one wavefront, and the
+request server with continuous batching over resident scenes. Every image must be bit-identical to
+the same work rendered alone: a path depends only on (scene, camera, pixel, sample index, seed,
+options), and each pixel's samples are summed in sample order."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from photon_b200 import abi, native
+import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _view(cam, w, h, spp, seed, depth=8):
+    return abi.View(cam, w, h, spp, seed, abi.path_options(max_depth=depth))
+
+
+def test_batched_views_equal_individual_renders():
+    desc, camf, keep = scenes.scene("terrain")
+    sizes = [(64, 36, 4, 1), (96, 54, 1, 2), (40, 30, 16, 3), (128, 72, 2, 4), (33, 17, 8, 5)]
+    views = []
+    for k, (w, h, spp, seed) in enumerate(sizes):
+        cam = camf(w / h)
+        cam.position.x += 0.3 * k
+        views.append(_view(cam, w, h, spp, seed, depth=12))
+    r = native.Renderer()
+    r.upload(desc)
+    r.render_views(views)
+    batched = [r.download_view(k, v.width, v.height) for k, v in enumerate(views)]
+    for k, v in enumerate(views):
+        r.resize(v.width, v.height)
+        r.reset()
+        r.render(v.camera, abi.RenderSettings(v.width, v.height, v.path, 1.0, abi.PT_TONEMAP_ACES, v.seed), v.spp)
+        alone = r.download_image()
+        assert np.array_equal(batched[k].view(np.uint32), alone.view(np.uint32)), f"view {k}"
+    r.close()
+
+
+def test_batched_views_with_split_passes_are_unchanged():
+    # A view bigger than one pass's radiance buffer is split by sample range; the per-pixel sums
+    # stay in sample order, so the image is unchanged.
+    desc, camf, keep = scenes.scene("box")
+    cam = camf(1.0)
+    r = native.Renderer()
+    r.upload(desc)
+    v = _view(cam, 64, 64, 32, 9)
+    r.render_views([v])
+    one = r.download_view(0, 64, 64)
+    r.resize(64, 64)
+    r.reset()
+    for _ in range(4):
+        r.render(cam, abi.render_settings(64, 64, seed=9), 8)
+    ref = O.orc_render(desc, cam, abi.render_settings(64, 64, seed=9), 32)
+    assert np.abs(one - ref).max() < 1e-3 * max(1.0, float(ref.max()))
+    r.close()
+
+
+@pytest.fixture(scope="module")
+def server_scenes():
+    box = scenes.scene("box")
+    terrain = scenes.scene("terrain")
+    return box, terrain
+
+
+def test_server_results_are_identical_alone_and_in_a_mix(server_scenes):
+    (bdesc, bcam, bkeep), (tdesc, tcam, tkeep) = server_scenes
+    s = native.Server(budget_bytes=8 << 30, path_capacity=1 << 18)
+    sb = s.add_scene(bdesc)
+    st = s.add_scene(tdesc)
+    probe = dict(scene_id=st, cam=tcam(96 / 54), w=96, h=54, spp=8, seed=11, path=abi.path_options(max_depth=12))
+    rid = s.submit(probe["scene_id"], probe["cam"], probe["w"], probe["h"], probe["spp"], probe["seed"], probe["path"])
+    s.wait(rid, 60)
+    alone, stats = s.fetch(rid, 96, 54)
+    assert stats.state == abi.PT_REQ_DONE and stats.samples == 96 * 54 * 8
+    # The same request among others of both scenes, submitted from several threads.
+    ids = []
+    lock = threading.Lock()
+
+    def submit_many(k):
+        for j in range(4):
+            sid = sb if (k + j) % 2 else st
+            cam = bcam(1.0) if sid == sb else tcam(16 / 9)
+            w, h = (48, 48) if sid == sb else (80, 45)
+            r = s.submit(sid, cam, w, h, 1 + 3 * j, 100 + 10 * k + j, abi.path_options(max_depth=8))
+            with lock:
+                ids.append((r, w, h))
+
+    threads = [threading.Thread(target=submit_many, args=(k,)) for k in range(3)]
+    for t in threads:
+        t.start()
+    rid2 = s.submit(probe["scene_id"], probe["cam"], probe["w"], probe["h"], probe["spp"], probe["seed"], probe["path"])
+    for t in threads:
+        t.join()
+    s.wait(rid2, 120)
+    mixed, _ = s.fetch(rid2, 96, 54)
+    assert np.array_equal(alone.view(np.uint32), mixed.view(np.uint32))
+    for r, w, h in ids:
+        s.wait(r, 120)
+        img, st_ = s.fetch(r, w, h)
+        assert st_.state == abi.PT_REQ_DONE and np.isfinite(img).all()
+    # ... and equal to the plain renderer's image of the same request.
+    rr = native.Renderer()
+    rr.upload(tdesc)
+    rr.resize(96, 54)
+    rr.render(probe["cam"], abi.RenderSettings(96, 54, probe["path"], 1.0, abi.PT_TONEMAP_ACES, 11), 8)
+    assert np.array_equal(rr.download_image().view(np.uint32), alone.view(np.uint32))
+    rr.close()
+    stats = s.stats()
+    assert stats.completed == 2 + len(ids) and stats.active == 0 and stats.queued == 0
+    s.close()
+
+
+def test_server_budget_cancel_and_faults(server_scenes):
+    (bdesc, bcam, bkeep), _ = server_scenes
+    budget = 256 << 20
+    s = native.Server(budget_bytes=budget, path_capacity=1 << 16)
+    sid = s.add_scene(bdesc)
+    cam = bcam(1.0)
+    # A request that can never fit the budget is refused at submission.
+    with pytest.raises(native.PhotonError) as e:
+        s.submit(sid, cam, 4096, 4096, 64)
+    assert e.value.code == abi.PT_ERR_BUDGET
+    assert s.stats().rejected == 1
+    # Unknown scene.
+    with pytest.raises(native.PhotonError) as e:
+        s.submit(sid + 7, cam, 8, 8, 1)
+    assert e.value.code == abi.PT_ERR_NOT_FOUND
+    # Host-side fault injection: the next allocation fails; that request fails, the server stays up.
+    s.fail_allocations(1)
+    bad = s.submit(sid, cam, 32, 32, 1)
+    with pytest.raises(native.PhotonError):
+        s.wait(bad, 30)
+    assert s.poll(bad) == abi.PT_REQ_FAILED
+    good = s.submit(sid, cam, 32, 32, 2)
+    s.wait(good, 30)
+    assert s.poll(good) == abi.PT_REQ_DONE
+    # Cancel a long request while it runs, and others (running or still queued); all end cancelled
+    # and their buffers are released.
+    big = s.submit(sid, cam, 256, 256, 128, path=abi.path_options(max_depth=64, rr_depth=64))
+    more = [s.submit(sid, cam, 256, 256, 64, path=abi.path_options(max_depth=64, rr_depth=64)) for _ in range(3)]
+    time.sleep(0.05)
+    for r in [big] + more:
+        s.cancel(r)
+    for r in [big] + more:
+        with pytest.raises(native.PhotonError) as e:
+            s.wait(r, 60)
+        assert e.value.code == abi.PT_ERR_CANCELLED
+        assert s.poll(r) == abi.PT_REQ_CANCELLED
+    # A wait that runs out reports a timeout instead of hanging.
+    slow = s.submit(sid, cam, 256, 256, 64)
+    with pytest.raises(native.PhotonError) as e:
+        s.wait(slow, 0.0)
+    assert e.value.code in (abi.PT_ERR_TIMEOUT,)
+    s.wait(slow, 60)
+    st = s.stats()
+    assert st.device_bytes_in_use <= budget
+    s.close()
