@@ -315,6 +315,24 @@ int32_t pt_svgf_run(pt_svgf* s, const float* color, const float* albedo, const f
 const float* pt_svgf_variance(const pt_svgf* s);
 const char* pt_svgf_last_error(const pt_svgf* s);
 
+/* An allocation-free SVGF denoise of one frame, for callers that cannot call cudaMalloc: an engine
+ * whose frame loop must not allocate (allocation synchronises the device and stalls the frame), a
+ * caller whose device memory is owned by its own caching allocator, code recorded into CUDA graphs
+ * or run where allocation is not allowed. No counterpart in Photon (its Svgf allocates its buffers in
+ * Svgf::resize, svgf.cu:225-236).
+ * The frame is denoised without history, as the first frame of a session (demodulate, spatial
+ * variance, `settings->atrous_iterations` a-trous passes, remodulate); inputs and output are caller
+ * device pointers to width*height float4 in the layout of pt_svgf_run. The intermediates live in one
+ * static device array of 32 MiB (524,288 pixels x 4 float4) that every GPU loading the library keeps
+ * until the process exits; frames above 524,288 pixels are rejected with PT_ERR_INVALID. The first
+ * call on a device looks up that array's device address (cudaGetSymbolAddress), so make it before any
+ * stream capture. The call only enqueues work on `stream` (a cudaStream_t, 0 = legacy default stream)
+ * and allocates nothing; every call shares the one array, so calls whose work overlaps on the GPU
+ * (other streams, other threads) race — order them on one stream. */
+int32_t pt_svgf_run_noalloc(int32_t device, int32_t width, int32_t height, const float* color, const float* albedo,
+                            const float* normal_depth, const float* position, const float* emission,
+                            const pt_svgf_settings* settings, float* output, void* stream);
+
 /* ---- request server (continuous batching over resident scenes) ------------------------------ */
 typedef struct pt_server pt_server;
 typedef struct pt_server_config {

@@ -275,6 +275,16 @@ const float* pt_svgf_variance(const pt_svgf* s) { return s ? s->s->variance() : 
 
 const char* pt_svgf_last_error(const pt_svgf* s) { return s ? s->error.c_str() : g_error.c_str(); }
 
+int32_t pt_svgf_run_noalloc(int32_t device, int32_t width, int32_t height, const float* color, const float* albedo,
+                            const float* normal_depth, const float* position, const float* emission, const pt_svgf_settings* settings,
+                            float* output, void* stream) {
+    if (!color || !albedo || !normal_depth || !position || !emission || !settings || !output) return PT_ERR_INVALID;
+    return guarded(nullptr, [&] {
+        svgf_run_noalloc(device, width, height, color, albedo, normal_depth, position, emission, *settings, output,
+                         reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
 // ---- server ------------------------------------------------------------------------------------------------
 
 int32_t pt_server_create(const pt_server_config* cfg, pt_server** out) {

@@ -7,6 +7,7 @@
 #include "svgf.h"
 
 #include <cstring>
+#include <mutex>
 
 #include "pt_math.cuh"
 
@@ -244,6 +245,20 @@ __global__ void k_history_remodulate(Frame5 in, int w, int h, const float4* __re
     }
 }
 
+// Remodulation alone (svgf.cu:199-210), for zero a-trous iterations without history.
+__global__ void k_remodulate_only(Frame5 in, int w, int h, const float4* __restrict__ filtered, float4* __restrict__ out) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    int i = y * w + x;
+    if (__ldg(in.pos + i).w < 0) {
+        out[i] = __ldg(in.color + i);
+        return;
+    }
+    V3 a = xyz(__ldg(in.albedo + i));
+    V3 c = xyz(__ldg(filtered + i)) * vmax(a, v3(1e-3f)) + xyz(__ldg(in.emission + i));
+    out[i] = make_float4(c.x, c.y, c.z, 1.0f);
+}
+
 }  // namespace
 
 SvgfDenoiser::SvgfDenoiser(int device, cudaStream_t stream) : device_(device), stream_(stream) {}
@@ -295,6 +310,73 @@ void SvgfDenoiser::run(const float* color, const float* albedo, const float* nd,
     }
     PTW_CUDA(cudaGetLastError());
     has_history_ = true;
+}
+
+// ---- the allocation-free single-frame denoise ------------------------------------------------------------
+// For callers that cannot allocate device memory (pt_svgf_run_noalloc): a frame is denoised without
+// history (the first frame of a session: demodulation, the spatial variance estimate, the a-trous
+// passes, remodulation) by the same kernels as SvgfDenoiser::run, with their four intermediate
+// buffers carved out of one file-scope device array instead of allocations.
+namespace {
+
+// illum, moments and the two a-trous buffers, kNoAllocMaxPixels float4 each: 32 MiB per device.
+static __device__ __align__(256) float4 g_noalloc_scratch[4 * size_t(kNoAllocMaxPixels)];
+
+std::mutex g_noalloc_mu;
+float4* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// The device address of the scratch array on the current device (host code must not use the
+// symbol's host-side name as a device pointer). Looked up once per device.
+float4* noalloc_scratch(int device) {
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        PTW_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[device] = static_cast<float4*>(p);
+    }
+    return g_noalloc_ptr[device];
+}
+
+}  // namespace
+
+void svgf_run_noalloc(int device, int w, int h, const float* color, const float* albedo, const float* nd, const float* pos,
+                      const float* emission, const pt_svgf_settings& s, float* output, cudaStream_t stream) {
+    if (w <= 0 || h <= 0) throw Error{PT_ERR_INVALID, "svgf_run_noalloc: width and height must be positive"};
+    if (int64_t(w) * int64_t(h) > kNoAllocMaxPixels)
+        throw Error{PT_ERR_INVALID, "svgf_run_noalloc: the frame has more than 524288 pixels (the size of the static scratch)"};
+    if (s.atrous_iterations < 0 || s.atrous_iterations > 30) throw Error{PT_ERR_INVALID, "atrous_iterations out of range"};
+    if (device < 0 || device >= kNoAllocMaxDevices) throw Error{PT_ERR_INVALID, "svgf_run_noalloc: device ordinal out of range"};
+    int previous = 0;
+    PTW_CUDA(cudaGetDevice(&previous));
+    PTW_CUDA(cudaSetDevice(device));
+    try {
+        float4* base = noalloc_scratch(device);
+        float4 *illum = base, *moments = base + kNoAllocMaxPixels, *f0 = base + 2 * size_t(kNoAllocMaxPixels),
+               *f1 = base + 3 * size_t(kNoAllocMaxPixels);
+        Frame5 in{reinterpret_cast<const float4*>(color), reinterpret_cast<const float4*>(albedo), reinterpret_cast<const float4*>(nd),
+                  reinterpret_cast<const float4*>(pos), reinterpret_cast<const float4*>(emission)};
+        PrevCamera pc{};  // unused without history
+        dim3 block(32, 4), grid((w + 31) / 32, (h + 3) / 4);
+        // Without history the temporal step reads nothing from earlier calls, and every scratch
+        // element a kernel reads was written earlier in this call: nothing needs clearing.
+        k_temporal<<<grid, block, 0, stream>>>(in, pc, w, h, 0, s.alpha_color, s.alpha_moments, nullptr, nullptr, nullptr, nullptr, illum,
+                                               moments);
+        k_variance<<<grid, block, 0, stream>>>(in, w, h, illum, moments, s.phi_normal, f0);
+        float4* bufs[2] = {f0, f1};
+        int src = 0;
+        for (int it = 0; it < s.atrous_iterations; it++) {
+            AtrousEpilogue ep{};
+            if (it == s.atrous_iterations - 1) ep.output = reinterpret_cast<float4*>(output);
+            k_atrous<<<grid, block, 0, stream>>>(in, w, h, 1 << it, s.phi_color, s.phi_normal, s.phi_depth, bufs[src], bufs[1 - src], ep);
+            src = 1 - src;
+        }
+        if (s.atrous_iterations == 0) k_remodulate_only<<<grid, block, 0, stream>>>(in, w, h, bufs[src], reinterpret_cast<float4*>(output));
+        PTW_CUDA(cudaGetLastError());
+    } catch (...) {
+        cudaSetDevice(previous);
+        throw;
+    }
+    PTW_CUDA(cudaSetDevice(previous));
 }
 
 }  // namespace ptw

@@ -31,4 +31,10 @@ private:
     DeviceBuffer<float4> prev_illum_, prev_moments_, prev_nd_, prev_pos_, illum_, moments_, filter_[2];
 };
 
+// The allocation-free single-frame denoise (pt_svgf_run_noalloc): scratch in a static device array.
+constexpr int kNoAllocMaxPixels = 1 << 19;  // 524,288 pixels (e.g. 960x540 or 1024x512)
+constexpr int kNoAllocMaxDevices = 64;
+void svgf_run_noalloc(int device, int w, int h, const float* color, const float* albedo, const float* normal_depth, const float* position,
+                      const float* emission, const pt_svgf_settings& s, float* output, cudaStream_t stream);
+
 }  // namespace ptw

@@ -70,6 +70,8 @@ def _load():
                          P(abi.SvgfSettings), C.c_void_p], C.c_int32),
         "pt_svgf_variance": ([C.c_void_p], C.c_void_p),
         "pt_svgf_last_error": ([C.c_void_p], C.c_char_p),
+        "pt_svgf_run_noalloc": ([C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 P(abi.SvgfSettings), C.c_void_p, C.c_void_p], C.c_int32),
         "pt_server_create": ([P(abi.ServerConfig), P(C.c_void_p)], C.c_int32),
         "pt_server_destroy": ([C.c_void_p], None),
         "pt_server_last_error": ([C.c_void_p], C.c_char_p),
@@ -279,6 +281,13 @@ class Svgf:
 
     def __del__(self):
         self.close()
+
+
+def svgf_run_noalloc(width, height, color, albedo, normal_depth, position, emission, settings, output, stream=0, device=0):
+    """The allocation-free single-frame SVGF denoise (pt_svgf_run_noalloc). Pointer arguments are
+    device addresses (ints) of width*height float4 buffers; the call enqueues on `stream`."""
+    _check(lib.pt_svgf_run_noalloc(device, width, height, color, albedo, normal_depth, position, emission, C.byref(settings),
+                                   output, stream), lib.pt_global_error)
 
 
 class Server:
