@@ -189,7 +189,7 @@ def systems_sections(r, g, desc, rank):
     - batched: 64 seeded views (320x180..1920x1080, spp {1,4,16,64}, cameras on a sphere of radius
       1.5x the scene extent) in one pt_render_views call, against the same views rendered one
       pt_render call at a time;
-    - served: a Poisson stream of 200 requests at 20 req/s over the 36-triangle box and the 262K scene
+    - served: a Poisson stream of 400 requests at 40 req/s over the 36-triangle box and the 262K scene
       (resolution / spp / depth drawn as in the serving configuration) through the server, against
       the same stream rendered one request at a time in arrival order; p50/p99 latency from
       submission to result."""
@@ -214,14 +214,14 @@ def systems_sections(r, g, desc, rank):
     server = native.Server(budget_bytes=150 << 30)
     sid_b = server.add_scene(bb.desc)
     sid_t = server.add_scene(desc)
-    stream = workloads.request_stream([(sid_b, bb.desc), (sid_t, desc)], 200, 20.0, seed=7)
+    stream = workloads.request_stream([(sid_b, bb.desc), (sid_t, desc)], 400, 40.0, seed=7)
     served = serving.run_served(server, stream)
     server.close()
     rb = native.Renderer(r_device(r))
     rb.upload(bb.desc)
     plain = serving.run_plain({sid_b: rb, sid_t: r}, stream)
     rb.close()
-    out["served"] = {"workload": "Poisson, 200 requests at 20 req/s, seed 7, scenes: 36-triangle box + 262K terrain",
+    out["served"] = {"workload": "Poisson, 400 requests at 40 req/s, seed 7, scenes: 36-triangle box + 262K terrain",
                      "served": served, "plain": plain, "budget_bytes": 150 << 30}
     return out
 
@@ -296,7 +296,8 @@ def main():
     samples_per_step = WIDTH * HEIGHT * SPP
     value = world * args.steps * samples_per_step / (total_ms / 1000.0) / 1e6
 
-    # End to end through the C ABI: render + download into a host buffer, wall clock.
+    # End to end through the C ABI: render + download into a host buffer, wall clock (no profiling).
+    r.set_profiling(0)
     e2e_t = []
     host = np.zeros((HEIGHT, WIDTH, 3), np.float32)
     for _ in range(args.steps):

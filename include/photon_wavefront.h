@@ -234,7 +234,8 @@ typedef struct pt_tuning {
     int32_t path_capacity;     /* paths in flight */
     int32_t trace_block;       /* threads per block of the traversal kernels */
     int32_t shade_block;       /* threads per block of the shading kernel */
-    int32_t sort_by_material;  /* reserved (0) */
+    int32_t sort_by_material;  /* k in 1-4: the shading kernel groups windows of k x shade_block paths by material
+                                  class before shading them; 0: queue order; -1 keep */
     int32_t graph_bounces;     /* bounce iterations captured per CUDA graph launch */
     int32_t sort_rays;         /* 0 off, 1-4: sort continuing rays by direction octant + Morton origin cell
                                   with this many bits per axis before tracing them; -1 keep */
@@ -242,7 +243,7 @@ typedef struct pt_tuning {
 } pt_tuning;
 int32_t pt_set_tuning(pt_renderer* r, const pt_tuning* t);
 int32_t pt_get_tuning(const pt_renderer* r, pt_tuning* t);
-/* The autotuner: picks path capacity, block shapes, graph cadence and ray sorting for the uploaded
+/* The autotuner: picks path capacity, block shapes, material sorting, graph cadence and ray sorting for the uploaded
  * scene by coordinate descent, timing probe renders of `camera` (at most `probe_samples` paths each,
  * into private buffers: the accumulation is untouched). Applies the best tuning, returns it in
  * `chosen` (optional) and the probe throughput of the default and chosen tunings (samples/s). */

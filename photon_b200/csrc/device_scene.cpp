@@ -87,7 +87,7 @@ size_t DeviceScene::device_bytes() const {
     return nodes_.bytes() + tris_.bytes() + normals_.bytes() + tangents_.bytes() + materials_.bytes() + alias_.bytes() +
            punctual_.bytes() + env_texels_.bytes() + tri_idx_.bytes() + textures_.bytes() + uvs_.bytes() + texels_.bytes() +
            srgb_lut_.bytes() + env_marginal_.bytes() + env_conditional_.bytes() + env_row_sin_.bytes() + emissive_.bytes() +
-           d_view_.bytes();
+           shade_keys_.bytes() + d_view_.bytes();
 }
 
 void DeviceScene::upload(const pt_scene_desc& d, cudaStream_t s, bool lights_only) {
@@ -125,6 +125,21 @@ void DeviceScene::upload(const pt_scene_desc& d, cudaStream_t s, bool lights_onl
     // and the environment.
     tris_.upload(reinterpret_cast<const float4*>(d.tris), size_t(d.num_tris) * 3, s);
     materials_.upload(reinterpret_cast<const float4*>(d.materials), size_t(d.num_materials) * 5, s);
+    // Shading classes: materials of one class take the same branches through the BSDF, texture and
+    // emission code, so the shade kernel groups a block's paths by class.
+    std::vector<uint8_t> keys(size_t(d.num_materials));
+    for (size_t m = 0; m < keys.size(); m++) {
+        const pt_material& mm = d.materials[m];
+        int k = 1;
+        if (mm.metallic > 0.0f) k += 1;
+        if (mm.transmission > 0.0f) k += 2;
+        if (mm.base_color_tex >= 0 || mm.metallic_roughness_tex >= 0) k += 4;
+        if (mm.normal_tex >= 0) k += 8;
+        if (mm.emission.x > 0.0f || mm.emission.y > 0.0f || mm.emission.z > 0.0f || mm.emissive_tex >= 0) k += 16;
+        keys[m] = uint8_t(k);
+    }
+    shade_keys_.upload(keys.data(), keys.size(), s);
+    PTW_CUDA(cudaStreamSynchronize(s));
     std::vector<int4> idx(size_t(d.num_tris));
     for (size_t t = 0; t < idx.size(); t++)
         idx[t] = make_int4(d.indices[3 * t], d.indices[3 * t + 1], d.indices[3 * t + 2], d.tri_emissive ? d.tri_emissive[t] : -1);
@@ -159,6 +174,7 @@ void DeviceScene::upload(const pt_scene_desc& d, cudaStream_t s, bool lights_onl
     v.uvs = uvs_.ptr;
     v.tangents = tangents_.ptr;
     v.materials = materials_.ptr;
+    v.shade_keys = shade_keys_.ptr;
     v.textures = textures_.ptr;
     v.texels = texels_.ptr;
     v.srgb_lut = srgb_lut_.ptr;

@@ -95,6 +95,7 @@ private:
     DeviceBuffer<int4> tri_idx_, textures_;
     DeviceBuffer<float2> uvs_;
     DeviceBuffer<uint32_t> texels_;
+    DeviceBuffer<uint8_t> shade_keys_;
     DeviceBuffer<float> srgb_lut_, env_marginal_, env_conditional_, env_row_sin_;
     DeviceBuffer<int2> emissive_;
     DeviceBuffer<DevScene> d_view_;

@@ -92,93 +92,145 @@ PT_HD float box_entry2(float4 bmin, float4 bmax, const RayPairs& r, float tmax) 
     return tnear <= tfar ? tnear : kInf;
 }
 
-// One traversal (traverse.h:66-138): nearest-first, leaves tested in place, `stack` is this thread's
-// column of the block's shared stack (entry k at stack[k * stride]). AnyHit stops at the first
-// accepted triangle. Packed selects the f32x2 slab test (bit-identical results).
+// Photon's traversal (traverse.h:66-138) as a state machine advanced one unit per step: a node visit
+// (both child slabs) or one triangle test. At each node both children are tested against the current
+// tmax; leaf children are then tested in place, side 0 first, and only after their triangles (which may
+// lower tmax) does the node push its farther interior child (if nearer than tmax and the 64-entry stack
+// has room) and descend to the nearer one (if nearer than tmax), or pop. Ties keep side 0 first. So the
+// sequence of node visits and triangle tests per ray, and the resulting hit, are Photon's.
+// Stepping one triangle at a time lets a lane that walks a leaf test one triangle while its
+// neighbours visit nodes, instead of every lane of the warp idling through the longest leaf loop.
 template <bool AnyHit, bool Count, bool Packed = true>
-PT_HD bool traverse(const DevScene& s, V3 o, V3 d, float tmax, Hit& hit, int* stack, int stride, TraversalCounters* cnt) {
-    V3 inv_d{safe_inv(d.x), safe_inv(d.y), safe_inv(d.z)};
-    RayPairs rp = ray_pairs(o, inv_d);
-    int overflow[kStackSize - kSmemStack];
-    int sp = 0;
-    int node = 0;
-    bool found = false;
-    const float4* nodes = s.nodes;
-    const float4* tris = s.tris;
-    while (true) {
-        const float4* n = nodes + 4 * node;
-        float4 n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2), n3 = __ldg(n + 3);
-        if (Count) cnt->nodes++;
-        float tl = Packed ? box_entry2(n0, n1, rp, tmax) : box_entry(n0, n1, o, inv_d, tmax);
-        float tr = Packed ? box_entry2(n2, n3, rp, tmax) : box_entry(n2, n3, o, inv_d, tmax);
-        int next0 = 0, next1 = 0;
-        float tn0 = 0, tn1 = 0;
-        int nn = 0;
-#pragma unroll
-        for (int side = 0; side < 2; side++) {
-            float tc = side == 0 ? tl : tr;
-            if (tc == kInf) continue;
-            int count = __float_as_int(side == 0 ? n1.w : n3.w);
-            int idx = __float_as_int(side == 0 ? n0.w : n2.w);
-            if (count > 0) {
-                for (int i = idx; i < idx + count; i++) {
-                    const float4* g = tris + 3 * i;
-                    float4 g0 = __ldg(g), g1 = __ldg(g + 1), g2 = __ldg(g + 2);
-                    float t, u, v;
-                    if (Count) cnt->tris++;
-                    if (tri_intersect(g0, g1, g2, o, d, tmax, t, u, v)) {
-                        if ((__float_as_int(g1.w) & 1) && alpha_passes(s, i, __float_as_int(g0.w), u, v)) continue;
-                        if (AnyHit) {
-                            hit.t = t;
-                            hit.tri = i;
-                            return true;
-                        }
-                        tmax = t;
-                        hit.t = t;
-                        hit.tri = i;
-                        hit.u = u;
-                        hit.v = v;
-                        found = true;
-                    }
-                }
-            } else if (idx >= 0) {
-                if (nn == 0) {
-                    next0 = idx;
-                    tn0 = tc;
-                } else {
-                    next1 = idx;
-                    tn1 = tc;
-                }
-                nn++;
+struct Walker {
+    V3 o, d, inv_d;
+    RayPairs rp;
+    float tmax;
+    int node;        // the node to visit next; -1 once the ray is finished
+    int sp;
+    int ti, te;      // leaf mode: the next triangle and the end of its range
+    int t1, e1;      // the second leaf range waiting behind the first (t1 == e1: none)
+    int near, far;   // inner children waiting for the leaf tests (-1: none)
+    float tn_near, tn_far;
+    bool leaf_mode;
+    int tri;         // closest (or first accepted) triangle, -1 for none; its distance is tmax
+    float u, v;
+
+    PT_HD void init(V3 o_, V3 d_, float tmax_) {
+        o = o_;
+        d = d_;
+        inv_d = V3{safe_inv(d.x), safe_inv(d.y), safe_inv(d.z)};
+        rp = ray_pairs(o, inv_d);
+        tmax = tmax_;
+        node = 0;
+        sp = 0;
+        ti = te = t1 = e1 = 0;
+        near = far = -1;
+        tn_near = tn_far = 0.0f;
+        leaf_mode = false;
+        tri = -1;
+        u = v = 0.0f;
+    }
+
+    // Advances one unit; returns false once the ray is finished.
+    PT_HD bool step(const DevScene& s, int* stack, int stride, int* overflow, TraversalCounters* cnt) {
+        bool decide = false;
+        if (!leaf_mode) {
+            const float4* n = s.nodes + 4 * node;
+            float4 n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2), n3 = __ldg(n + 3);
+            if (Count) cnt->nodes++;
+            float tl = Packed ? box_entry2(n0, n1, rp, tmax) : box_entry(n0, n1, o, inv_d, tmax);
+            float tr = Packed ? box_entry2(n2, n3, rp, tmax) : box_entry(n2, n3, o, inv_d, tmax);
+            int c0 = __float_as_int(n1.w), i0 = __float_as_int(n0.w), c1 = __float_as_int(n3.w), i1 = __float_as_int(n2.w);
+            bool h0 = tl != kInf, h1 = tr != kInf;
+            bool leaf0 = h0 && c0 > 0, leaf1 = h1 && c1 > 0;
+            bool in0 = h0 && c0 <= 0 && i0 >= 0, in1 = h1 && c1 <= 0 && i1 >= 0;
+            // Inner children in side order, then nearest first (a tie keeps side 0 first).
+            near = in0 ? i0 : (in1 ? i1 : -1);
+            tn_near = in0 ? tl : tr;
+            far = (in0 && in1) ? i1 : -1;
+            tn_far = tr;
+            if (far >= 0 && tn_near > tn_far) {
+                int a = near;
+                near = far;
+                far = a;
+                float b = tn_near;
+                tn_near = tn_far;
+                tn_far = b;
+            }
+            if (leaf0 || leaf1) {
+                ti = leaf0 ? i0 : i1;
+                te = leaf0 ? i0 + c0 : i1 + c1;
+                bool both = leaf0 && leaf1;
+                t1 = both ? i1 : 0;
+                e1 = both ? i1 + c1 : 0;
+                leaf_mode = true;
+            } else {
+                decide = true;
             }
         }
-        if (nn == 2) {
-            if (tn0 > tn1) {
-                int a = next0;
-                next0 = next1;
-                next1 = a;
-                float b = tn0;
-                tn0 = tn1;
-                tn1 = b;
+        if (leaf_mode) {
+            int i = ti;
+            const float4* g = s.tris + 3 * i;
+            float4 g0 = __ldg(g), g1 = __ldg(g + 1), g2 = __ldg(g + 2);
+            float t, tu, tv;
+            if (Count) cnt->tris++;
+            if (tri_intersect(g0, g1, g2, o, d, tmax, t, tu, tv) &&
+                !((__float_as_int(g1.w) & 1) && alpha_passes(s, i, __float_as_int(g0.w), tu, tv))) {
+                tmax = t;
+                tri = i;
+                u = tu;
+                v = tv;
+                if (AnyHit) {
+                    node = -1;
+                    return false;
+                }
             }
-            if (tn1 < tmax && sp < kStackSize) {
-                if (sp < kSmemStack) stack[sp * stride] = next1;
-                else overflow[sp - kSmemStack] = next1;
+            if (++ti == te) {
+                if (t1 != e1) {
+                    ti = t1;
+                    te = e1;
+                    t1 = e1 = 0;
+                } else {
+                    leaf_mode = false;
+                    decide = true;
+                }
+            }
+        }
+        if (decide) {
+            if (far >= 0 && tn_far < tmax && sp < kStackSize) {
+                if (sp < kSmemStack) stack[sp * stride] = far;
+                else overflow[sp - kSmemStack] = far;
                 sp++;
             }
-            if (tn0 < tmax) {
-                node = next0;
-                continue;
+            if (near >= 0 && tn_near < tmax) {
+                node = near;
+            } else if (sp == 0) {
+                node = -1;
+            } else {
+                --sp;
+                node = sp < kSmemStack ? stack[sp * stride] : overflow[sp - kSmemStack];
             }
-        } else if (nn == 1 && tn0 < tmax) {
-            node = next0;
-            continue;
         }
-        if (sp == 0) break;
-        --sp;
-        node = sp < kSmemStack ? stack[sp * stride] : overflow[sp - kSmemStack];
+        return node >= 0;
     }
-    return found;
+};
+
+// One ray's traversal: AnyHit stops at the first accepted triangle. `stack` is this thread's column of
+// the block's shared stack (entry k at stack[k * stride]).
+template <bool AnyHit, bool Count, bool Packed = true>
+PT_HD bool traverse(const DevScene& s, V3 o, V3 d, float tmax, Hit& hit, int* stack, int stride, TraversalCounters* cnt) {
+    int overflow[kStackSize - kSmemStack];
+    Walker<AnyHit, Count, Packed> w;
+    w.init(o, d, tmax);
+    while (w.step(s, stack, stride, overflow, cnt)) {
+    }
+    if (w.tri >= 0) {
+        hit.t = w.tmax;
+        hit.tri = w.tri;
+        hit.u = w.u;
+        hit.v = w.v;
+    }
+    return w.tri >= 0;
 }
 
 }  // namespace ptw

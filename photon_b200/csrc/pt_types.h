@@ -23,6 +23,7 @@ struct DevScene {
     const float2* uvs;
     const float4* tangents;
     const float4* materials;
+    const uint8_t* shade_keys;  // per material: its shading class (1..32) for the material-sorted shade
     const int4* textures;
     const uint32_t* texels;
     const float* srgb_lut;

@@ -126,6 +126,7 @@ WfParams WavefrontEngine::params(const DevScene* scenes, int single, const DevVi
     p.count_work = count ? 1 : 0;
     p.packed = tuning_.packed ? 1 : 0;
     p.sort_bits = tuning_.sort_rays;
+    p.sort_material = tuning_.sort_by_material;
     p.keys = keys_.ptr;
     p.hist = hist_.ptr;
     p.offsets = offsets_.ptr;
@@ -577,7 +578,10 @@ void Renderer::set_tuning(const pt_tuning& t) {
         if (t.shade_block % 32 || t.shade_block > 256) throw Error{PT_ERR_INVALID, "shade_block must be a multiple of 32, at most 256"};
         cur.shade_block = t.shade_block;
     }
-    if (t.sort_by_material >= 0) cur.sort_by_material = t.sort_by_material;
+    if (t.sort_by_material >= 0) {
+        if (t.sort_by_material > 4) throw Error{PT_ERR_INVALID, "sort_by_material must be in [0, 4]"};
+        cur.sort_by_material = t.sort_by_material;
+    }
     if (t.graph_bounces >= 0) cur.graph_bounces = t.graph_bounces;
     if (t.sort_rays >= 0) {
         if (t.sort_rays > 4) throw Error{PT_ERR_INVALID, "sort_rays must be in [0, 4]"};
@@ -596,7 +600,6 @@ void Renderer::get_tuning(pt_tuning* t) const {
     t->graph_bounces = c.graph_bounces;
     t->sort_rays = c.sort_rays;
     t->packed = c.packed;
-    t->sort_by_material = 0;
 }
 
 // Coordinate descent over the knobs, one at a time, each candidate timed on the same probe (a view
@@ -650,6 +653,7 @@ void Renderer::autotune(const pt_camera& cam, const pt_render_settings& rs, int 
     try_knob([](Tuning& t, int v) { t.path_capacity = v; }, {1 << 19, 1 << 20, 1 << 21, 1 << 22});
     try_knob([](Tuning& t, int v) { t.trace_block = v; }, {64, 128, 256});
     try_knob([](Tuning& t, int v) { t.shade_block = v; }, {64, 128, 256});
+    try_knob([](Tuning& t, int v) { t.sort_by_material = v; }, {0, 1, 2, 4});
     try_knob([](Tuning& t, int v) { t.graph_bounces = v; }, {2, 4, 8});
     try_knob([](Tuning& t, int v) { t.sort_rays = v; }, {0, 3});
     engine_->set_tuning(best);

@@ -18,8 +18,8 @@ class SvgfDenoiser;
 struct Tuning {
     int path_capacity = 1 << 21;   // paths in flight
     int trace_block = 128;
-    int shade_block = 128;
-    int sort_by_material = 0;
+    int shade_block = 256;
+    int sort_by_material = 4;      // shade windows of 4 x shade_block paths grouped by material class
     int graph_bounces = 4;         // iterations per CUDA graph launch
     int sort_rays = 0;             // origin bits per axis of the ray-sort key (0: no sorting)
     int packed = 1;                // f32x2 slab tests

@@ -216,14 +216,11 @@ __device__ __forceinline__ uint32_t ray_key(const DevScene& s, V3 o, V3 d, int b
 }
 
 // ---- shade: one vertex of trace_path (integrator.h:158-262) -----------------------------------------
-__global__ void __launch_bounds__(256) k_shade(const __grid_constant__ WfParams P) {
-    Counters* c = P.ctr;
-    const uint32_t p = c->parity, q = p ^ 1u, n = c->count[p];
-    for (;;) {
-        uint32_t i0 = warp_fetch(&c->fetch[2]);
-        if (i0 >= n) break;
-        uint32_t i = i0 + lane_id();
-        bool active = i < n;
+// Shades path `i` of the current queue (every lane of the warp calls it; `active` is false for lanes
+// without a path).
+__device__ __forceinline__ void shade_path(const WfParams& P, Counters* c, uint32_t p, uint32_t i, bool active) {
+    const uint32_t q = p ^ 1u;
+    {
         bool cont = false, shadow = false;
         // Path state.
         V3 ro{0, 0, 0}, rd{0, 0, 0}, beta{0, 0, 0}, L{0, 0, 0}, sh_o{0, 0, 0}, sh_d{0, 0, 0}, sh_c{0, 0, 0};
@@ -366,6 +363,77 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ WfParams 
                 if (dc) atomicAdd(dc, (unsigned long long)__popc(peers));
             }
         }
+    }
+}
+
+// The shading class of a queued path: 0 for a miss, else the class of the hit triangle's material
+// (1..32, precomputed per material at upload from its lobes, textures and emission).
+constexpr uint32_t kShadeKeys = 64;
+__device__ __forceinline__ uint32_t shade_key(const WfParams& P, uint32_t p, uint32_t i) {
+    int tri = __float_as_int(P.pb.hit[i].y);
+    if (tri < 0) return 0;
+    const DevScene& s = scene_for(P, P.single_scene >= 0 ? 0 : int(P.pb.id[p][i].x));
+    return s.shade_keys[__float_as_int(__ldg(s.tris + 3 * tri).w)];
+}
+
+// Persistent over the queue. Without material sorting each warp claims 32 paths in queue order. With
+// it each block claims a window of sort_material x blockDim paths, orders them by shading class in
+// shared memory (a counting sort on 64 keys) and shades them in that order, so a warp mostly runs one
+// BSDF lobe and one texture pattern. The order in which paths are shaded changes only where their
+// outputs are appended, not any path's result.
+constexpr int kMaxShadeRounds = 4;  // sort_material <= 4 and window <= 1024 paths
+constexpr uint32_t kMaxShadeWindow = 1024;
+__global__ void __launch_bounds__(256) k_shade(const __grid_constant__ WfParams P) {
+    Counters* c = P.ctr;
+    const uint32_t p = c->parity, n = c->count[p];
+    if (!P.sort_material) {
+        for (;;) {
+            uint32_t i0 = warp_fetch(&c->fetch[2]);
+            if (i0 >= n) break;
+            uint32_t i = i0 + lane_id();
+            shade_path(P, c, p, i, i < n);
+        }
+        return;
+    }
+    __shared__ uint32_t s_base, s_hist[kShadeKeys], s_perm[kMaxShadeWindow];
+    const uint32_t tid = threadIdx.x, window = uint32_t(P.sort_material) * blockDim.x;
+    for (;;) {
+        if (tid == 0) s_base = atomicAdd(&c->fetch[2], window);
+        for (uint32_t k = tid; k < kShadeKeys; k += blockDim.x) s_hist[k] = 0;
+        __syncthreads();
+        const uint32_t i0 = s_base;
+        if (i0 >= n) break;
+        uint32_t key[kMaxShadeRounds], rank[kMaxShadeRounds];
+#pragma unroll
+        for (int r = 0; r < kMaxShadeRounds; r++) {
+            if (r < P.sort_material) {
+                const uint32_t i = i0 + uint32_t(r) * blockDim.x + tid;
+                key[r] = i < n ? shade_key(P, p, i) : kShadeKeys - 1;
+                rank[r] = atomicAdd(&s_hist[key[r]], 1u);
+            }
+        }
+        __syncthreads();
+        if (tid < 32) {  // exclusive scan of the 64 bucket counts, two per lane
+            uint32_t a = s_hist[2 * tid], b = s_hist[2 * tid + 1];
+            uint32_t incl = a + b;
+            for (int off = 1; off < 32; off <<= 1) {
+                uint32_t v = __shfl_up_sync(kFull, incl, off);
+                if (int(tid) >= off) incl += v;
+            }
+            uint32_t excl = incl - a - b;
+            s_hist[2 * tid] = excl;
+            s_hist[2 * tid + 1] = excl + a;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kMaxShadeRounds; r++)
+            if (r < P.sort_material) s_perm[s_hist[key[r]] + rank[r]] = i0 + uint32_t(r) * blockDim.x + tid;
+        __syncthreads();
+        for (int r = 0; r < P.sort_material; r++) {
+            const uint32_t j = s_perm[uint32_t(r) * blockDim.x + tid];
+            shade_path(P, c, p, j, j < n);
+        }
+        __syncthreads();
     }
 }
 

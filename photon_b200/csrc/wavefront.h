@@ -71,6 +71,7 @@ struct WfParams {
     Counters* ctr;
     int count_work;            // 1: count node visits / triangle tests (stats runs)
     int packed;                // 1: f32x2 slab tests in the traversal kernels
+    int sort_material;         // 1: the shade kernel groups each block's paths by material class
     int sort_bits;             // > 0: sort continuing paths by direction octant + Morton origin cell
                                //      (this many bits per axis) before they are traced
     uint32_t* keys;            // capacity entries (sort keys of the shade output)

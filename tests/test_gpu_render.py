@@ -198,3 +198,33 @@ def test_gpu_matches_golden_fixtures(renderer, name):
     renderer.render(cam, rs, spp)
     frac, ma, mb = pixel_agreement(z["image"], renderer.download_image())
     assert frac >= PIXEL_FRACTION and abs(ma - mb) <= MEAN_REL * ma
+
+
+@pytest.mark.parametrize("tuning", [
+    dict(packed=0),
+    dict(sort_by_material=0),
+    dict(sort_by_material=1, shade_block=128),
+    dict(sort_by_material=2, shade_block=64),
+    dict(sort_rays=3),
+    dict(trace_block=64, shade_block=64),
+    dict(path_capacity=1 << 14, graph_bounces=1),
+])
+def test_tuning_variants_are_bit_identical(tuning):
+    """Every autotuner knob changes how the work is scheduled, never a path's arithmetic: scalar or
+    packed slab tests, material-sorted shading, ray sorting, block shapes, the path pool size and the
+    graph cadence all give the same image bit for bit (accumulation is in sample order)."""
+    desc, camf, keep = scenes.scene("terrain")
+    w, h, spp = 160, 90, 4
+    cam = camf(w / h)
+    rs = _settings("terrain", w, h, seed=3)
+    imgs = []
+    for t in ({}, tuning):
+        r = native.Renderer()
+        r.upload(desc)
+        r.resize(w, h)
+        if t:
+            r.set_tuning(**t)
+        r.render(cam, rs, spp)
+        imgs.append(r.download_image())
+        r.close()
+    assert np.array_equal(imgs[0], imgs[1])
