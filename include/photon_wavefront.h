@@ -313,6 +313,11 @@ int32_t pt_svgf_run(pt_svgf* s, const float* color, const float* albedo, const f
                     const float* position, const float* emission, const pt_camera* previous,
                     const pt_svgf_settings* settings, float* output);
 /* The variance estimate of the last run (Svgf::variance_buffer, svgf.h:44): a device pointer. */
+/* How the a-trous passes read their 5x5 taps: 0 from global memory; 1 (default) from shared-memory
+ * tiles that the Tensor Memory Accelerator stages, contiguous tiles for steps 1-8 and global loads
+ * beyond; 2 as 1 plus a strided tile (one residue class of x, y mod 8) for step 16; 3 strided tiles
+ * for steps 1-16. Every mode gives the same output bit for bit. */
+int32_t pt_svgf_set_tma(pt_svgf* s, int32_t mode);
 const float* pt_svgf_variance(const pt_svgf* s);
 const char* pt_svgf_last_error(const pt_svgf* s);
 
@@ -324,7 +329,7 @@ const char* pt_svgf_last_error(const pt_svgf* s);
  * The frame is denoised without history, as the first frame of a session (demodulate, spatial
  * variance, `settings->atrous_iterations` a-trous passes, remodulate); inputs and output are caller
  * device pointers to width*height float4 in the layout of pt_svgf_run. The intermediates live in one
- * static device array of 32 MiB (524,288 pixels x 4 float4) that every GPU loading the library keeps
+ * static device array of 40 MiB (524,288 pixels x 5 float4) that every GPU loading the library keeps
  * until the process exits; frames above 524,288 pixels are rejected with PT_ERR_INVALID. The first
  * call on a device looks up that array's device address (cudaGetSymbolAddress), so make it before any
  * stream capture. The call only enqueues work on `stream` (a cudaStream_t, 0 = legacy default stream)

@@ -271,6 +271,11 @@ int32_t pt_svgf_run(pt_svgf* s, const float* color, const float* albedo, const f
     });
 }
 
+int32_t pt_svgf_set_tma(pt_svgf* s, int32_t mode) {
+    if (!s) return PT_ERR_INVALID;
+    return guarded(&s->error, [&] { s->s->set_tma(mode); });
+}
+
 const float* pt_svgf_variance(const pt_svgf* s) { return s ? s->s->variance() : nullptr; }
 
 const char* pt_svgf_last_error(const pt_svgf* s) { return s ? s->error.c_str() : g_error.c_str(); }

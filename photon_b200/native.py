@@ -70,6 +70,7 @@ def _load():
                          P(abi.SvgfSettings), C.c_void_p], C.c_int32),
         "pt_svgf_variance": ([C.c_void_p], C.c_void_p),
         "pt_svgf_last_error": ([C.c_void_p], C.c_char_p),
+        "pt_svgf_set_tma": ([C.c_void_p, C.c_int32], C.c_int32),
         "pt_svgf_run_noalloc": ([C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  P(abi.SvgfSettings), C.c_void_p, C.c_void_p], C.c_int32),
         "pt_server_create": ([P(abi.ServerConfig), P(C.c_void_p)], C.c_int32),
@@ -270,6 +271,10 @@ class Svgf:
 
     def reset(self):
         lib.pt_svgf_reset(self.h)
+
+    def set_tma(self, mode):
+        """0 global loads, 1-3 TMA-staged tiles (pt_svgf_set_tma)."""
+        _check(lib.pt_svgf_set_tma(self.h, int(mode)), lambda: lib.pt_svgf_last_error(self.h))
 
     def variance_ptr(self):
         return lib.pt_svgf_variance(self.h)

@@ -176,3 +176,26 @@ def test_denoised_gbuffer_is_the_oracle_sample(torch_cuda):
     assert np.array_equal(albedo.view(np.uint32), g["albedo"].view(np.uint32))
     assert np.array_equal(nd.view(np.uint32), g["normal_depth"].view(np.uint32))
     r.close()
+
+
+@pytest.mark.parametrize("w,h,iterations", [(101, 67, 5), (96, 64, 6), (40, 24, 3)])
+def test_tma_staged_passes_equal_direct_loads(torch_cuda, w, h, iterations):
+    """The a-trous passes that read TMA-staged shared-memory tiles (contiguous or strided) compute
+    exactly what the global-load passes compute: outputs are bit-identical frame after frame in every
+    staging mode, on sizes that are not multiples of the tile grid and with a pass beyond the staged
+    steps."""
+    torch = torch_cuda
+    cams, gbufs, keep = _frames("materials", w, h, 4)
+    settings = abi.svgf_settings()
+    settings.atrous_iterations = iterations
+    outs = []
+    for mode in (0, 1, 2, 3):
+        sv = native.Svgf(w, h)
+        sv.set_tma(mode)
+        outs.append(_run_device(torch, lambda d, prev, out: sv.run(d["color"].data_ptr(), d["albedo"].data_ptr(), d["normal_depth"].data_ptr(),
+                                                                   d["position"].data_ptr(), d["emission"].data_ptr(), prev, settings,
+                                                                   out.data_ptr()), cams, gbufs, w, h))
+        sv.close()
+    for staged in outs[1:]:
+        for a, b in zip(staged, outs[0]):
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
