@@ -240,10 +240,12 @@ typedef struct pt_tuning {
     int32_t sort_rays;         /* 0 off, 1-4: sort continuing rays by direction octant + Morton origin cell
                                   with this many bits per axis before tracing them; -1 keep */
     int32_t packed;            /* 1: f32x2 (packed FP32) slab tests in traversal, 0: scalar; -1 keep */
+    int32_t tail_paths;        /* once no new paths remain and at most this many are queued, one kernel finishes
+                                  them (a thread per path, every bounce); 0 never; -1 keep */
 } pt_tuning;
 int32_t pt_set_tuning(pt_renderer* r, const pt_tuning* t);
 int32_t pt_get_tuning(const pt_renderer* r, pt_tuning* t);
-/* The autotuner: picks path capacity, block shapes, material sorting, graph cadence and ray sorting for the uploaded
+/* The autotuner: picks path capacity, block shapes, material sorting, graph cadence, ray sorting and the tail size for the uploaded
  * scene by coordinate descent, timing probe renders of `camera` (at most `probe_samples` paths each,
  * into private buffers: the accumulation is untouched). Applies the best tuning, returns it in
  * `chosen` (optional) and the probe throughput of the default and chosen tunings (samples/s). */

@@ -116,7 +116,8 @@ void WavefrontEngine::ensure_shape() {
 }
 
 WfParams WavefrontEngine::params(const DevScene* scenes, int single, const DevView* views, int n, bool count) const {
-    WfParams p{};
+    WfParams p;
+    std::memset(&p, 0, sizeof(p));  // padding too: captured graphs are matched by comparing the bytes
     p.scenes = scenes;
     p.views = views;
     p.num_views = n;
@@ -127,6 +128,7 @@ WfParams WavefrontEngine::params(const DevScene* scenes, int single, const DevVi
     p.packed = tuning_.packed ? 1 : 0;
     p.sort_bits = tuning_.sort_rays;
     p.sort_material = tuning_.sort_by_material;
+    p.tail_paths = uint32_t(tuning_.tail_paths);
     p.keys = keys_.ptr;
     p.hist = hist_.ptr;
     p.offsets = offsets_.ptr;
@@ -279,7 +281,7 @@ void Renderer::resize(int w, int h) {
     width_ = w;
     height_ = h;
     size_t n = size_t(w) * size_t(h);
-    for (DeviceBuffer<float4>* b : {&accum_, &albedo_, &normal_depth_, &position_, &emission_, &color_, &denoised_buf_}) {
+    for (DeviceBuffer<float4>* b : {&accum_, &albedo_, &normal_depth_, &edge_, &motion_, &emission_, &color_, &denoised_buf_}) {
         b->allocate(n);
         b->zero(stream_);
     }
@@ -450,17 +452,23 @@ void Renderer::render_denoised(const pt_camera& cam, const pt_camera& prev, cons
     v.accum = acc_pass_.ptr;
     v.g_albedo = albedo_.ptr;
     v.g_normal_depth = normal_depth_.ptr;
-    v.g_position = position_.ptr;
     v.g_emission = emission_.ptr;
     v.g_color = color_.ptr;
+    // The denoiser's own records: octahedral normal + depth + material, and the reprojection into
+    // the previous camera's image.
+    v.g_edge = edge_.ptr;
+    v.g_motion = motion_.ptr;
+    static_assert(sizeof(v.prev_cam) == sizeof(pt_camera), "camera layout");
+    std::memcpy(v.prev_cam, &prev, sizeof(v.prev_cam));
+    v.has_prev = 1;
     std::vector<DevView> views{v};
     std::vector<int> spps{1};
     std::vector<uint32_t> f0{frame_};
     PTW_CUDA(cudaEventRecord(ev0_, stream_));
     render_pass_set(views, 1, spps, f0);
-    svgf_->run(reinterpret_cast<const float*>(color_.ptr), reinterpret_cast<const float*>(albedo_.ptr),
-               reinterpret_cast<const float*>(normal_depth_.ptr), reinterpret_cast<const float*>(position_.ptr),
-               reinterpret_cast<const float*>(emission_.ptr), prev, sv, reinterpret_cast<float*>(denoised_buf_.ptr));
+    svgf_->run_frame(reinterpret_cast<const float*>(color_.ptr), reinterpret_cast<const float*>(albedo_.ptr),
+                     reinterpret_cast<const float*>(emission_.ptr), reinterpret_cast<const float*>(edge_.ptr),
+                     reinterpret_cast<const float*>(motion_.ptr), sv, reinterpret_cast<float*>(denoised_buf_.ptr));
     PTW_CUDA(cudaEventRecord(ev1_, stream_));
     PTW_CUDA(cudaEventSynchronize(ev1_));
     cudaEventElapsedTime(&last_ms_, ev0_, ev1_);
@@ -547,7 +555,7 @@ void Renderer::stats(pt_stats* out) const {
     out->bounce_iterations = last_ctr_.iterations;
     out->queue_overflows = last_ctr_.overflow;
     size_t b = scene_.device_bytes() + engine_->device_bytes() + sample_out_.bytes() + heat_.bytes() + display_.bytes();
-    for (const DeviceBuffer<float4>* x : {&accum_, &acc_pass_, &albedo_, &normal_depth_, &position_, &emission_, &color_, &denoised_buf_}) b += x->bytes();
+    for (const DeviceBuffer<float4>* x : {&accum_, &acc_pass_, &albedo_, &normal_depth_, &edge_, &motion_, &emission_, &color_, &denoised_buf_}) b += x->bytes();
     out->device_bytes = b;
 }
 
@@ -588,6 +596,7 @@ void Renderer::set_tuning(const pt_tuning& t) {
         cur.sort_rays = t.sort_rays;
     }
     if (t.packed >= 0) cur.packed = t.packed ? 1 : 0;
+    if (t.tail_paths >= 0) cur.tail_paths = t.tail_paths;
     engine_->set_tuning(cur);
 }
 
@@ -600,6 +609,7 @@ void Renderer::get_tuning(pt_tuning* t) const {
     t->graph_bounces = c.graph_bounces;
     t->sort_rays = c.sort_rays;
     t->packed = c.packed;
+    t->tail_paths = c.tail_paths;
 }
 
 // Coordinate descent over the knobs, one at a time, each candidate timed on the same probe (a view
@@ -656,6 +666,7 @@ void Renderer::autotune(const pt_camera& cam, const pt_render_settings& rs, int 
     try_knob([](Tuning& t, int v) { t.sort_by_material = v; }, {0, 1, 2, 4});
     try_knob([](Tuning& t, int v) { t.graph_bounces = v; }, {2, 4, 8});
     try_knob([](Tuning& t, int v) { t.sort_rays = v; }, {0, 3});
+    try_knob([](Tuning& t, int v) { t.tail_paths = v; }, {0, 1 << 16, 1 << 18, 1 << 20});
     engine_->set_tuning(best);
     batch_views_ = saved_views;
     if (tuned_rate) *tuned_rate = best_rate;

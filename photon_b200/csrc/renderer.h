@@ -23,6 +23,7 @@ struct Tuning {
     int graph_bounces = 4;         // iterations per CUDA graph launch
     int sort_rays = 0;             // origin bits per axis of the ray-sort key (0: no sorting)
     int packed = 1;                // f32x2 slab tests
+    int tail_paths = 1 << 18;      // finish the last queued paths one thread each below this many (0: never)
 };
 
 // Runs wavefront passes over a table of views on one device stream. Owns the path pool, the
@@ -144,7 +145,7 @@ private:
     uint32_t frame_ = 0;
     float last_ms_ = 0;
     bool denoised_ = false;
-    DeviceBuffer<float4> accum_, acc_pass_, albedo_, normal_depth_, position_, emission_, color_, denoised_buf_;
+    DeviceBuffer<float4> accum_, acc_pass_, albedo_, normal_depth_, edge_, motion_, emission_, color_, denoised_buf_;
     DeviceBuffer<float> heat_;
     DeviceBuffer<uint32_t> display_;
     DeviceBuffer<float4> sample_out_;

@@ -12,15 +12,13 @@
 #include <cstring>
 #include <mutex>
 
+#include "gbuffer.cuh"
 #include "pt_math.cuh"
 
 namespace ptw {
 
 namespace {
 
-struct PrevCamera {
-    float c[16];  // pt_camera
-};
 
 // Photon's SvgfInput (svgf.h:24-30): five float4 per pixel.
 struct Frame5 {
@@ -37,20 +35,6 @@ struct SvgfFrame {
     const float4 *color, *albedo, *emission, *edge, *motion;
 };
 
-__device__ __forceinline__ float sign_nz(float v) { return v < 0.0f ? -1.0f : 1.0f; }
-
-// Octahedral normal encoding (Meyer et al. 2010; Cigolle et al. 2014), FP32.
-__device__ __forceinline__ float2 oct_encode(V3 n) {
-    float s = fabsf(n.x) + fabsf(n.y) + fabsf(n.z);
-    if (!(s > 0.0f)) return make_float2(0.0f, 0.0f);
-    float px = n.x / s, py = n.y / s;
-    if (n.z < 0.0f) {
-        float qx = (1.0f - fabsf(py)) * sign_nz(px), qy = (1.0f - fabsf(px)) * sign_nz(py);
-        px = qx;
-        py = qy;
-    }
-    return make_float2(px, py);
-}
 // The octahedral map's unnormalised direction; oct_decode normalises it (the fast reciprocal square
 // root is accurate to a few ulp, far inside the filter's tolerances).
 __device__ __forceinline__ V3 oct_direction(float ex, float ey) {
@@ -80,20 +64,6 @@ __device__ __forceinline__ V3 demodulate(V3 color, V3 emission, V3 albedo) {
     return {il.x / fmaxf(albedo.x, 1e-3f), il.y / fmaxf(albedo.y, 1e-3f), il.z / fmaxf(albedo.z, 1e-3f)};
 }
 
-// project (svgf.cu:25-35): a world position in the previous frame's pixel coordinates.
-__device__ __forceinline__ bool project(const PrevCamera& pc, V3 p, int w, int h, float& px, float& py, float& dist) {
-    const float* c = pc.c;
-    V3 d = p - V3{c[0], c[1], c[2]};
-    float z = dot(d, V3{c[4], c[5], c[6]});
-    if (z <= 1e-4f) return false;
-    float sx = dot(d, V3{c[8], c[9], c[10]}) / (z * c[3] * c[7]);
-    float sy = dot(d, V3{c[12], c[13], c[14]}) / (z * c[3]);
-    px = (sx + 1.0f) * 0.5f * float(w) - 0.5f;
-    py = (1.0f - sy) * 0.5f * float(h) - 0.5f;
-    dist = length(d);
-    return true;
-}
-
 struct History {
     const float4 *illum, *moments, *edge;  // the previous frame's
 };
@@ -114,8 +84,7 @@ __global__ void __launch_bounds__(128) k_temporal(Frame5 in5, SvgfFrame in, Prev
     float px = 0, py = 0, dist = 0;
     if (FromPhoton) {
         float4 nd = __ldg(in5.nd + i), pos = __ldg(in5.pos + i);
-        float2 o = oct_encode(xyz(nd));
-        edge = make_float4(o.x, o.y, nd.w, __int_as_float(int(pos.w)));
+        edge = edge_record(xyz(nd), nd.w, int(pos.w));
         edge_out[i] = edge;
         color = xyz(__ldg(in5.color + i));
         albedo = xyz(__ldg(in5.albedo + i));

@@ -16,6 +16,7 @@
 // warp until the iteration's count (read from device memory) is exhausted. Compiled with
 // -fmad=false and IEEE division / square root: see pt_math.cuh.
 #include "wavefront.h"
+#include "gbuffer.cuh"
 
 #include "pt_traverse.cuh"
 
@@ -110,7 +111,7 @@ __device__ __forceinline__ int find_view(const DevView* views, int n, unsigned l
 }
 
 // ---- setup ------------------------------------------------------------------------------------------
-__global__ void k_setup(Counters* c, uint32_t capacity) {
+__global__ void k_setup(Counters* c, uint32_t capacity, uint32_t tail_paths) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     uint32_t p = c->parity ^ 1u;
     c->parity = p;
@@ -127,6 +128,7 @@ __global__ void k_setup(Counters* c, uint32_t capacity) {
     c->shadow_rays += c->shadow_count;
     c->shadow_count = 0;
     c->rays += cnt + n;
+    c->tail = (tail_paths > 0 && cnt + n > 0 && cnt + n <= tail_paths && c->work_next >= c->work_total) ? 1u : 0u;
     for (int k = 0; k < 6; k++) c->fetch[k] = 0;
     if (cnt + n > 0) c->iterations++;
 }
@@ -170,6 +172,7 @@ __global__ void __launch_bounds__(256) k_trace(const __grid_constant__ WfParams 
     extern __shared__ int smem_stack[];
     int* stack = smem_stack + threadIdx.x;
     Counters* c = P.ctr;
+    if (c->tail) return;
     const uint32_t p = c->parity, n = c->count[p];
     TraversalCounters tc{0, 0};
     for (;;) {
@@ -216,152 +219,194 @@ __device__ __forceinline__ uint32_t ray_key(const DevScene& s, V3 o, V3 d, int b
 }
 
 // ---- shade: one vertex of trace_path (integrator.h:158-262) -----------------------------------------
-// Shades path `i` of the current queue (every lane of the warp calls it; `active` is false for lanes
-// without a path).
+struct PathState {
+    V3 ro, rd, beta, L;
+    float prev_pdf;
+    uint32_t flags;  // depth | prev_delta << 16
+    uint4 id;        // (view, local work index, pixel, sample in pass)
+    Rng rng;
+};
+struct ShadowRay {
+    V3 o, d, c;
+    float tmax;
+};
+
+__device__ __forceinline__ PathState load_path(const WfParams& P, uint32_t p, uint32_t i) {
+    PathState st;
+    float4 o4 = P.pb.o[p][i], d4 = P.pb.d[p][i], b4 = P.pb.beta[p][i], l4 = P.pb.lr[p][i];
+    st.id = P.pb.id[p][i];
+    st.ro = xyz(o4);
+    st.rd = xyz(d4);
+    st.prev_pdf = o4.w;
+    st.flags = __float_as_uint(d4.w);
+    st.beta = xyz(b4);
+    st.L = V3{b4.w, l4.x, l4.y};
+    st.rng.state = uint64_t(__float_as_uint(l4.z)) | (uint64_t(__float_as_uint(l4.w)) << 32);
+    st.rng.inc = (uint64_t(st.id.z) << 1u) | 1u;
+    return st;
+}
+
+// One vertex of trace_path for a path whose closest hit is h4 = (t, tri, u, v): adds the emitted
+// light it sees to st.L, writes the first vertex's G-buffer, samples the light (a shadow ray in *sh
+// when `shadow` comes back true) and the continuation (st's ray, throughput and flags). Returns
+// whether the path continues.
+__device__ __forceinline__ bool shade_vertex(const WfParams& P, PathState& st, float4 h4, bool& shadow, ShadowRay& sh) {
+    const uint4 id = st.id;
+    const DevView& v = P.views[id.x];
+    const DevScene& s = scene_for(P, id.x);
+    V3& ro = st.ro;
+    V3& rd = st.rd;
+    V3& beta = st.beta;
+    V3& L = st.L;
+    float& prev_pdf = st.prev_pdf;
+    Rng& rng = st.rng;
+    bool cont = false;
+    shadow = false;
+    int depth = int(st.flags & 0xffffu);
+    bool prev_delta = (st.flags >> 16) & 1u;
+    int tri = __float_as_int(h4.y);
+    bool gbuf = v.gbuffer && id.w == 0 && depth == 0;
+    if (tri < 0) {
+        // Miss: the environment, weighted against light sampling (integrator.h:159-177).
+        V3 le = env_radiance(s, rd);
+        float w = (prev_delta || s.p_env <= 0) ? 1.0f : power_heuristic(prev_pdf, env_pdf(s, rd));
+        V3 cc = beta * le * w;
+        clamp_contribution(cc, depth, v.clamp);
+        L = L + cc;
+        if (gbuf) {
+            V3 pos = ro + rd * 1e4f;
+            v.g_albedo[id.z] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+            v.g_normal_depth[id.z] = make_float4(-rd.x, -rd.y, -rd.z, 0.0f);
+            if (v.g_position) v.g_position[id.z] = make_float4(pos.x, pos.y, pos.z, -1.0f);
+            if (v.g_emission) v.g_emission[id.z] = make_float4(le.x, le.y, le.z, 1.0f);
+            if (v.g_edge) {
+                v.g_edge[id.z] = edge_record(-rd, 0.0f, -1);
+                v.g_motion[id.z] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
+        }
+        return false;
+    }
+    Interaction it = surface_at(s, ro, rd, h4.x, tri, h4.z, h4.w);
+    V3 wo_world = -rd;
+    if (!is_black(it.emission)) {
+        float w = 1.0f;
+        if (!prev_delta) w = power_heuristic(prev_pdf, emissive_pdf(s, tri, it.emissive_entry, rd, h4.x));
+        V3 cc = beta * it.emission * w;
+        clamp_contribution(cc, depth, v.clamp);
+        L = L + cc;
+    }
+    Bsdf bsdf = make_bsdf(it.params);
+    if (gbuf) {
+        V3 alb = bsdf_albedo(bsdf);
+        v.g_albedo[id.z] = make_float4(alb.x, alb.y, alb.z, 1.0f);
+        v.g_normal_depth[id.z] = make_float4(it.ns.x, it.ns.y, it.ns.z, h4.x);
+        if (v.g_position) v.g_position[id.z] = make_float4(it.p.x, it.p.y, it.p.z, float(it.material));
+        if (v.g_emission) v.g_emission[id.z] = make_float4(it.emission.x, it.emission.y, it.emission.z, 1.0f);
+        if (v.g_edge) {
+            const int px = int(id.z % uint32_t(v.width)), py = int(id.z / uint32_t(v.width));
+            v.g_edge[id.z] = edge_record(it.ns, h4.x, it.material);
+            v.g_motion[id.z] = motion_record(*reinterpret_cast<const PrevCamera*>(v.prev_cam), v.has_prev != 0, it.p, it.material, px, py,
+                                             v.width, v.height);
+        }
+    }
+    if (depth + 1 >= v.max_depth) return false;
+    V3 wo = to_local(it.frame, wo_world);
+    bool nee = v.nee && s.has_lights && samples_lights(bsdf);
+    if (nee) {
+        float ug = rng_next(rng);
+        V2 ul = rng_next2(rng);
+        float uk = rng_next(rng);
+        LightSample ls = sample_light(s, it.p, ug, ul, uk, nullptr);
+        if (ls.pdf > 0 && !is_black(ls.radiance)) {
+            V3 wi = to_local(it.frame, ls.wi);
+            float pdf_b;
+            V3 f = bsdf_eval_pdf(bsdf, wo, wi, &pdf_b);
+            if (!is_black(f)) {
+                sh.o = offset_ray(it.p, dot(ls.wi, it.ng) > 0 ? it.ng : -it.ng);
+                sh.d = ls.wi;
+                sh.tmax = ls.dist == kInf ? kInf : ls.dist * (1.0f - 1e-4f);
+                float w = ls.delta ? 1.0f : power_heuristic(ls.pdf, pdf_b);
+                sh.c = beta * f * fabsf(wi.z) * ls.radiance * (w / ls.pdf);
+                clamp_contribution(sh.c, depth, v.clamp);
+                shadow = true;
+            }
+        }
+    }
+    float u_lobe = rng_next(rng);
+    V2 u = rng_next2(rng);
+    float u_sub = rng_next(rng);
+    BsdfSample bs = bsdf_sample(bsdf, wo, u_lobe, u, u_sub);
+    if (bs.valid) {
+        beta = beta * (bs.f * (fabsf(bs.wi.z) / bs.pdf));
+        if (is_finite(beta) && !is_black(beta)) {
+            V3 wi_world = to_world(it.frame, bs.wi);
+            float side = dot(wi_world, it.ng) * dot(wo_world, it.ng);
+            if (!(bs.transmitted ? side >= 0 : side <= 0)) {
+                prev_pdf = bs.pdf;
+                ro = offset_ray(it.p, dot(wi_world, it.ng) > 0 ? it.ng : -it.ng);
+                rd = normalize(wi_world);
+                cont = true;
+                if (depth + 1 >= v.rr_depth) {
+                    float qq = fmaxf(0.05f, 1.0f - max_component(beta));
+                    if (rng_next(rng) < qq) cont = false;
+                    else beta = beta * (1.0f / (1.0f - qq));
+                }
+                st.flags = uint32_t(depth + 1) | ((nee ? 0u : 1u) << 16);
+            }
+        }
+    }
+    return cont;
+}
+
+// Shades path `i` of the current queue and appends its continuation and shadow ray to the next
+// queues (every lane of the warp calls it; `active` is false for lanes without a path).
 __device__ __forceinline__ void shade_path(const WfParams& P, Counters* c, uint32_t p, uint32_t i, bool active) {
     const uint32_t q = p ^ 1u;
-    {
-        bool cont = false, shadow = false;
-        // Path state.
-        V3 ro{0, 0, 0}, rd{0, 0, 0}, beta{0, 0, 0}, L{0, 0, 0}, sh_o{0, 0, 0}, sh_d{0, 0, 0}, sh_c{0, 0, 0};
-        float prev_pdf = 0, sh_tmax = 0;
-        uint32_t flags = 0;
-        uint4 id = make_uint4(0, 0, 0, 0);
-        Rng rng{0, 1};
-        if (active) {
-            float4 o4 = P.pb.o[p][i], d4 = P.pb.d[p][i], b4 = P.pb.beta[p][i], l4 = P.pb.lr[p][i], h4 = P.pb.hit[i];
-            id = P.pb.id[p][i];
-            const DevView& v = P.views[id.x];
-            const DevScene& s = scene_for(P, id.x);
-            ro = xyz(o4);
-            rd = xyz(d4);
-            prev_pdf = o4.w;
-            flags = __float_as_uint(d4.w);
-            int depth = int(flags & 0xffffu);
-            bool prev_delta = (flags >> 16) & 1u;
-            beta = xyz(b4);
-            L = V3{b4.w, l4.x, l4.y};
-            rng.state = uint64_t(__float_as_uint(l4.z)) | (uint64_t(__float_as_uint(l4.w)) << 32);
-            rng.inc = (uint64_t(id.z) << 1u) | 1u;
-            int tri = __float_as_int(h4.y);
-            bool gbuf = v.gbuffer && id.w == 0 && depth == 0;
-            if (tri < 0) {
-                // Miss: the environment, weighted against light sampling (integrator.h:159-177).
-                V3 le = env_radiance(s, rd);
-                float w = (prev_delta || s.p_env <= 0) ? 1.0f : power_heuristic(prev_pdf, env_pdf(s, rd));
-                V3 cc = beta * le * w;
-                clamp_contribution(cc, depth, v.clamp);
-                L = L + cc;
-                if (gbuf) {
-                    V3 pos = ro + rd * 1e4f;
-                    v.g_albedo[id.z] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-                    v.g_normal_depth[id.z] = make_float4(-rd.x, -rd.y, -rd.z, 0.0f);
-                    if (v.g_position) v.g_position[id.z] = make_float4(pos.x, pos.y, pos.z, -1.0f);
-                    if (v.g_emission) v.g_emission[id.z] = make_float4(le.x, le.y, le.z, 1.0f);
-                }
-            } else {
-                Interaction it = surface_at(s, ro, rd, h4.x, tri, h4.z, h4.w);
-                V3 wo_world = -rd;
-                if (!is_black(it.emission)) {
-                    float w = 1.0f;
-                    if (!prev_delta) w = power_heuristic(prev_pdf, emissive_pdf(s, tri, it.emissive_entry, rd, h4.x));
-                    V3 cc = beta * it.emission * w;
-                    clamp_contribution(cc, depth, v.clamp);
-                    L = L + cc;
-                }
-                Bsdf bsdf = make_bsdf(it.params);
-                if (gbuf) {
-                    V3 alb = bsdf_albedo(bsdf);
-                    v.g_albedo[id.z] = make_float4(alb.x, alb.y, alb.z, 1.0f);
-                    v.g_normal_depth[id.z] = make_float4(it.ns.x, it.ns.y, it.ns.z, h4.x);
-                    if (v.g_position) v.g_position[id.z] = make_float4(it.p.x, it.p.y, it.p.z, float(it.material));
-                    if (v.g_emission) v.g_emission[id.z] = make_float4(it.emission.x, it.emission.y, it.emission.z, 1.0f);
-                }
-                if (depth + 1 < v.max_depth) {
-                    V3 wo = to_local(it.frame, wo_world);
-                    bool nee = v.nee && s.has_lights && samples_lights(bsdf);
-                    if (nee) {
-                        float ug = rng_next(rng);
-                        V2 ul = rng_next2(rng);
-                        float uk = rng_next(rng);
-                        LightSample ls = sample_light(s, it.p, ug, ul, uk, nullptr);
-                        if (ls.pdf > 0 && !is_black(ls.radiance)) {
-                            V3 wi = to_local(it.frame, ls.wi);
-                            float pdf_b;
-                            V3 f = bsdf_eval_pdf(bsdf, wo, wi, &pdf_b);
-                            if (!is_black(f)) {
-                                sh_o = offset_ray(it.p, dot(ls.wi, it.ng) > 0 ? it.ng : -it.ng);
-                                sh_d = ls.wi;
-                                sh_tmax = ls.dist == kInf ? kInf : ls.dist * (1.0f - 1e-4f);
-                                float w = ls.delta ? 1.0f : power_heuristic(ls.pdf, pdf_b);
-                                sh_c = beta * f * fabsf(wi.z) * ls.radiance * (w / ls.pdf);
-                                clamp_contribution(sh_c, depth, v.clamp);
-                                shadow = true;
-                            }
-                        }
-                    }
-                    float u_lobe = rng_next(rng);
-                    V2 u = rng_next2(rng);
-                    float u_sub = rng_next(rng);
-                    BsdfSample bs = bsdf_sample(bsdf, wo, u_lobe, u, u_sub);
-                    if (bs.valid) {
-                        beta = beta * (bs.f * (fabsf(bs.wi.z) / bs.pdf));
-                        if (is_finite(beta) && !is_black(beta)) {
-                            V3 wi_world = to_world(it.frame, bs.wi);
-                            float side = dot(wi_world, it.ng) * dot(wo_world, it.ng);
-                            if (!(bs.transmitted ? side >= 0 : side <= 0)) {
-                                prev_pdf = bs.pdf;
-                                ro = offset_ray(it.p, dot(wi_world, it.ng) > 0 ? it.ng : -it.ng);
-                                rd = normalize(wi_world);
-                                cont = true;
-                                if (depth + 1 >= v.rr_depth) {
-                                    float qq = fmaxf(0.05f, 1.0f - max_component(beta));
-                                    if (rng_next(rng) < qq) cont = false;
-                                    else beta = beta * (1.0f / (1.0f - qq));
-                                }
-                                flags = uint32_t(depth + 1) | ((nee ? 0u : 1u) << 16);
-                            }
-                        }
-                    }
-                }
-            }
-        }
-        // Continuing paths move to the other buffer, compacted.
-        uint32_t slot = warp_append(cont, &c->count[q]);
-        if (P.sort_bits > 0) {
-            uint32_t key = cont ? ray_key(scene_for(P, id.x), ro, rd, P.sort_bits) : 0xffffffffu;
-            uint32_t peers = __match_any_sync(kFull, key);
-            if (cont) {
-                P.keys[slot] = key;
-                if (int(lane_id()) == __ffs(peers) - 1) atomicAdd(&P.hist[key], uint32_t(__popc(peers)));
-            }
-        }
+    bool cont = false, shadow = false;
+    PathState st;
+    ShadowRay sh;
+    if (active) {
+        st = load_path(P, p, i);
+        cont = shade_vertex(P, st, P.pb.hit[i], shadow, sh);
+    } else {
+        st.id = make_uint4(0, 0, 0, 0);
+    }
+    const uint4 id = st.id;
+    // Continuing paths move to the other buffer, compacted.
+    uint32_t slot = warp_append(cont, &c->count[q]);
+    if (P.sort_bits > 0) {
+        uint32_t key = cont ? ray_key(scene_for(P, id.x), st.ro, st.rd, P.sort_bits) : 0xffffffffu;
+        uint32_t peers = __match_any_sync(kFull, key);
         if (cont) {
-            P.pb.o[q][slot] = make_float4(ro.x, ro.y, ro.z, prev_pdf);
-            P.pb.d[q][slot] = make_float4(rd.x, rd.y, rd.z, __uint_as_float(flags));
-            P.pb.beta[q][slot] = make_float4(beta.x, beta.y, beta.z, L.x);
-            P.pb.lr[q][slot] = make_float4(L.y, L.z, __uint_as_float(uint32_t(rng.state)), __uint_as_float(uint32_t(rng.state >> 32)));
-            P.pb.id[q][slot] = id;
-        } else if (active) {
-            const DevView& v = P.views[id.x];
-            v.sample_out[id.y] = make_float4(L.x, L.y, L.z, 0.0f);
+            P.keys[slot] = key;
+            if (int(lane_id()) == __ffs(peers) - 1) atomicAdd(&P.hist[key], uint32_t(__popc(peers)));
         }
-        // Shadow rays: target the continuing slot, or the finished sample.
-        uint32_t qs = warp_append(shadow, &c->shadow_count);
-        if (shadow) {
-            P.pb.sh0[qs] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_tmax);
-            P.pb.sh1[qs] = make_float4(sh_d.x, sh_d.y, sh_d.z, __uint_as_float(cont ? slot : id.y));
-            P.pb.sh2[qs] = make_float4(sh_c.x, sh_c.y, sh_c.z, __uint_as_float(id.x | (cont ? 0u : 0x80000000u)));
-        }
-        // Progress of views that count finished paths (the request server).
-        bool finished = active && !cont;
-        if (P.num_views > 1 || P.views[0].done_counter) {
-            uint32_t key = finished ? id.x : 0xffffffffu;
-            uint32_t peers = __match_any_sync(kFull, key);
-            if (finished && int(lane_id()) == __ffs(peers) - 1) {
-                unsigned long long* dc = P.views[id.x].done_counter;
-                if (dc) atomicAdd(dc, (unsigned long long)__popc(peers));
-            }
+    }
+    if (cont) {
+        P.pb.o[q][slot] = make_float4(st.ro.x, st.ro.y, st.ro.z, st.prev_pdf);
+        P.pb.d[q][slot] = make_float4(st.rd.x, st.rd.y, st.rd.z, __uint_as_float(st.flags));
+        P.pb.beta[q][slot] = make_float4(st.beta.x, st.beta.y, st.beta.z, st.L.x);
+        P.pb.lr[q][slot] =
+            make_float4(st.L.y, st.L.z, __uint_as_float(uint32_t(st.rng.state)), __uint_as_float(uint32_t(st.rng.state >> 32)));
+        P.pb.id[q][slot] = id;
+    } else if (active) {
+        P.views[id.x].sample_out[id.y] = make_float4(st.L.x, st.L.y, st.L.z, 0.0f);
+    }
+    // Shadow rays: target the continuing slot, or the finished sample.
+    uint32_t qs = warp_append(shadow, &c->shadow_count);
+    if (shadow) {
+        P.pb.sh0[qs] = make_float4(sh.o.x, sh.o.y, sh.o.z, sh.tmax);
+        P.pb.sh1[qs] = make_float4(sh.d.x, sh.d.y, sh.d.z, __uint_as_float(cont ? slot : id.y));
+        P.pb.sh2[qs] = make_float4(sh.c.x, sh.c.y, sh.c.z, __uint_as_float(id.x | (cont ? 0u : 0x80000000u)));
+    }
+    // Progress of views that count finished paths (the request server).
+    bool finished = active && !cont;
+    if (P.num_views > 1 || P.views[0].done_counter) {
+        uint32_t key = finished ? id.x : 0xffffffffu;
+        uint32_t peers = __match_any_sync(kFull, key);
+        if (finished && int(lane_id()) == __ffs(peers) - 1) {
+            unsigned long long* dc = P.views[id.x].done_counter;
+            if (dc) atomicAdd(dc, (unsigned long long)__popc(peers));
         }
     }
 }
@@ -385,6 +430,7 @@ constexpr int kMaxShadeRounds = 4;  // sort_material <= 4 and window <= 1024 pat
 constexpr uint32_t kMaxShadeWindow = 1024;
 __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ WfParams P) {
     Counters* c = P.ctr;
+    if (c->tail) return;
     const uint32_t p = c->parity, n = c->count[p];
     if (!P.sort_material) {
         for (;;) {
@@ -437,12 +483,63 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ WfParams 
     }
 }
 
+// ---- tail: the last queued paths, each finished by one thread --------------------------------------------
+// Once no new paths remain and few are queued, an iteration's kernels have too little work to cover
+// the latency of their longest ray, and every remaining bounce would pay that again. k_tail takes the
+// whole queue instead: each thread traces, shades and shadow-tests its path bounce after bounce, in
+// the order of the queued kernels (emission, then the light sample's contribution, then the next
+// bounce), so each path's result is the same as through the queues.
+template <bool Count, bool Packed>
+__global__ void __launch_bounds__(256) k_tail(const __grid_constant__ WfParams P) {
+    Counters* c = P.ctr;
+    if (!c->tail) return;
+    extern __shared__ int smem_stack[];
+    int* stack = smem_stack + threadIdx.x;
+    const uint32_t p = c->parity, n = c->count[p];
+    TraversalCounters tc{0, 0}, ts{0, 0};
+    unsigned long long rays = 0, shadow_rays = 0;
+    for (;;) {
+        uint32_t i0 = warp_fetch(&c->fetch[5]);
+        if (i0 >= n) break;
+        uint32_t i = i0 + lane_id();
+        if (i >= n) continue;
+        PathState st = load_path(P, p, i);
+        const DevScene& s = scene_for(P, st.id.x);
+        for (bool first = true;; first = false) {
+            Hit h{kInf, -1, 0.0f, 0.0f};
+            traverse<false, Count, Packed>(s, st.ro, st.rd, kInf, h, stack, blockDim.x, &tc);
+            if (!first) rays++;  // the setup counted each queued path's first ray
+            bool shadow = false;
+            ShadowRay sh;
+            bool cont = shade_vertex(P, st, make_float4(h.t, __int_as_float(h.tri), h.u, h.v), shadow, sh);
+            if (shadow) {
+                Hit hs{kInf, -1, 0.0f, 0.0f};
+                shadow_rays++;
+                if (!traverse<true, Count, Packed>(s, sh.o, sh.d, sh.tmax, hs, stack, blockDim.x, &ts)) st.L = st.L + sh.c;
+            }
+            if (!cont) break;
+        }
+        const DevView& v = P.views[st.id.x];
+        v.sample_out[st.id.y] = make_float4(st.L.x, st.L.y, st.L.z, 0.0f);
+        if (v.done_counter) atomicAdd(v.done_counter, 1ull);
+    }
+    if (rays) atomicAdd(&c->rays, rays);
+    if (shadow_rays) atomicAdd(&c->shadow_rays, shadow_rays);
+    if (Count) {
+        warp_add_u64(&c->node_visits, tc.nodes);
+        warp_add_u64(&c->tri_tests, tc.tris);
+        warp_add_u64(&c->shadow_node_visits, ts.nodes);
+        warp_add_u64(&c->shadow_tri_tests, ts.tris);
+    }
+}
+
 // ---- shadow: any hit (traverse.h:144-147) --------------------------------------------------------------
 template <bool Count, bool Packed>
 __global__ void __launch_bounds__(256) k_shadow(const __grid_constant__ WfParams P) {
     extern __shared__ int smem_stack[];
     int* stack = smem_stack + threadIdx.x;
     Counters* c = P.ctr;
+    if (c->tail) return;
     const uint32_t q = c->parity ^ 1u, n = c->shadow_count;
     TraversalCounters tc{0, 0};
     for (;;) {
@@ -764,24 +861,43 @@ static void launch_traversal(const WfParams& p, const LaunchShape& ls, cudaStrea
     }
 }
 
+static void launch_tail(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, size_t smem) {
+    if (p.count_work) {
+        if (p.packed) k_tail<true, true><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
+        else k_tail<true, false><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
+    } else {
+        if (p.packed) k_tail<false, true><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
+        else k_tail<false, false><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
+    }
+}
+
 cudaError_t wf_iteration(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, cudaEvent_t* ev) {
     size_t smem = size_t(kSmemStack) * ls.trace_block * sizeof(int);
-    if (ev) cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
-    k_setup<<<1, 32, 0, stream>>>(p.ctr, p.pb.capacity);
-    if (ev) cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal);
+    // Timing events: inside a stream capture they must be external event nodes to be recorded at
+    // all; outside one they are ordinary records.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (ev) cudaStreamIsCapturing(stream, &cap);
+    const unsigned flags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
+    auto mark = [&](int k) {
+        if (ev) cudaEventRecordWithFlags(ev[k], stream, flags);
+    };
+    mark(0);
+    k_setup<<<1, 32, 0, stream>>>(p.ctr, p.pb.capacity, p.tail_paths);
+    mark(1);
     k_generate<<<ls.gen_grid, ls.gen_block, 0, stream>>>(p);
-    if (ev) cudaEventRecordWithFlags(ev[2], stream, cudaEventRecordExternal);
+    mark(2);
+    if (p.tail_paths > 0) launch_tail(p, ls, stream, smem);
     launch_traversal(p, ls, stream, smem, false);
-    if (ev) cudaEventRecordWithFlags(ev[3], stream, cudaEventRecordExternal);
+    mark(3);
     k_shade<<<ls.shade_grid, ls.shade_block, 0, stream>>>(p);
-    if (ev) cudaEventRecordWithFlags(ev[4], stream, cudaEventRecordExternal);
+    mark(4);
     launch_traversal(p, ls, stream, smem, true);
     if (p.sort_bits > 0) {
         k_sort_scan<<<1, 1024, 0, stream>>>(p, 8u << (3 * p.sort_bits));
         k_sort_scatter<<<ls.gen_grid, ls.gen_block, 0, stream>>>(p);
         k_sort_finish<<<1, 32, 0, stream>>>(p.ctr);
     }
-    if (ev) cudaEventRecordWithFlags(ev[5], stream, cudaEventRecordExternal);
+    mark(5);
     return cudaGetLastError();
 }
 

@@ -29,6 +29,10 @@ struct DevView {
     float4* g_position;
     float4* g_emission;
     float4* g_color;
+    float4* g_edge;           // the denoiser's edge and motion records (see gbuffer.cuh), optional
+    float4* g_motion;
+    float prev_cam[16];       // pt_camera of the previous frame, for the motion records
+    int has_prev;
     unsigned long long* done_counter;  // optional: paths finished (for serving progress)
 };
 
@@ -40,8 +44,9 @@ struct Counters {
     uint32_t count[2];               // paths in each buffer
     uint32_t shadow_count;
     uint32_t gen_base, gen_n;        // slots filled by this iteration's generate step
-    uint32_t fetch[6];               // work-claim counters: generate, trace, shade, shadow, sort scatter
+    uint32_t fetch[6];               // work-claim counters: generate, trace, shade, shadow, sort scatter, tail
     uint32_t overflow;
+    uint32_t tail;                   // 1: this iteration finishes every queued path in k_tail
     uint32_t iterations;
     unsigned long long work_base, work_next, work_total;
     unsigned long long rays, shadow_rays, paths_done;
@@ -71,6 +76,8 @@ struct WfParams {
     Counters* ctr;
     int count_work;            // 1: count node visits / triangle tests (stats runs)
     int packed;                // 1: f32x2 slab tests in the traversal kernels
+    uint32_t tail_paths;       // > 0: once no new paths remain and at most this many are queued, finish them
+                               // in one kernel (one thread per path, all bounces)
     int sort_material;         // 1: the shade kernel groups each block's paths by material class
     int sort_bits;             // > 0: sort continuing paths by direction octant + Morton origin cell
                                //      (this many bits per axis) before they are traced

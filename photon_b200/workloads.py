@@ -6,6 +6,8 @@
 - `request_stream`: a Poisson request stream for the server — resolution from {256^2, 640x360,
   1280x720, 1920x1080} with probabilities {0.4, 0.3, 0.2, 0.1}, spp from {1, 8, 64}, max depth from
   {4, 8, 12}, scenes uniformly.
+- `orbit_cameras`: the real-time sessions' camera paths — an orbit around the scene's centre,
+  0.5 degrees per frame.
 """
 import math
 
@@ -77,3 +79,15 @@ def request_stream(scenes, n, rate, seed=7):
         cam = sphere_camera(rng, center, extent, w / h)
         out.append(dict(t=t, scene=sid, cam=cam, w=w, h=h, spp=spp, seed=7000 + k, path=abi.path_options(max_depth=depth)))
     return out
+
+
+def orbit_cameras(desc, frames, aspect, start_deg=0.0, step_deg=0.5, radius=0.9, elevation=0.45, vfov=45.0):
+    """`frames` cameras on a circle of `radius` x the scene extent around its centre, `elevation` x the
+    extent above it, looking at the centre; consecutive cameras `step_deg` degrees apart."""
+    center, extent = scene_sphere(desc)
+    cams = []
+    for k in range(frames):
+        a = math.radians(start_deg + step_deg * k)
+        pos = center + extent * np.array([radius * math.cos(a), elevation, radius * math.sin(a)])
+        cams.append(look_at(pos, center, vfov, aspect))
+    return cams

@@ -121,3 +121,72 @@ def test_batched_views_vs_photon_megakernel(L):
     rec = {"batched_msamples_per_s": total / wf / 1e6, "megakernel_msamples_per_s": total / mk / 1e6, "speedup": mk / wf}
     print("BATCHED_VS_MEGAKERNEL " + json.dumps(rec))
     assert rec["speedup"] > 1.0
+
+
+def test_realtime_sessions_vs_photon(L, torch_cuda=None):
+    """Real-time frames (1 spp + G-buffer + SVGF) on an orbit of the 262K scene at 1600x900: one
+    session through pt_render_denoised against Photon's GpuRenderer::render_denoised (megakernel +
+    svgf.cu), and SVGF alone, ours against svgf.cu, on identical G-buffers. Frame times are wall clock
+    of the synchronous calls; percentiles over the orbit's frames."""
+    import torch
+    from photon_b200 import workloads
+    desc, camf, keep = scenes.scene("terrain")
+    W, H, N = 1600, 900, 40
+    cams = workloads.orbit_cameras(desc, N + 3, W / H)
+    rs = abi.render_settings(W, H, max_depth=12, seed=11)
+    sv = abi.svgf_settings()
+
+    def frame_times(step):
+        for f in range(3):
+            step(cams[f], cams[max(f - 1, 0)])
+        ts = []
+        for f in range(3, N + 3):
+            t0 = time.perf_counter()
+            step(cams[f], cams[f - 1])
+            ts.append((time.perf_counter() - t0) * 1e3)
+        return np.percentile(ts, 50), np.percentile(ts, 99)
+
+    r = native.Renderer()
+    r.upload(desc)
+    r.resize(W, H)
+    ours = frame_times(lambda c, p: r.render_denoised(c, p, rs, sv))
+    r.close()
+    ref_scene = O.RefScene.from_desc(desc, lib=L)
+    g = L.refgpu_create()
+    try:
+        assert L.refgpu_upload(g, ref_scene.h)
+        L.refgpu_resize(g, W, H)
+        theirs = frame_times(lambda c, p: L.refgpu_render_denoised(g, C.byref(c), C.byref(p), C.byref(rs), C.byref(sv)))
+    finally:
+        L.refgpu_destroy(g)
+    # SVGF alone on identical G-buffers (the oracle's first-vertex G-buffer of the first orbit frame).
+    gb = O.orc_gbuffer(desc, cams[0], abi.render_settings(W, H, seed=2), frame=0)
+    names = ("color", "albedo", "normal_depth", "position", "emission")
+    dev = {n: torch.from_numpy(gb[n]).cuda() for n in names}
+    out = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
+    ptrs = [dev[n].data_ptr() for n in names]
+
+    def device_ms(run, n=20):
+        for _ in range(3):
+            run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            run()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    ours_sv = native.Svgf(W, H)
+    svgf_ours = device_ms(lambda: ours_sv.run(*ptrs, cams[0], sv, out.data_ptr()))
+    ours_sv.close()
+    ref = L.refsvgf_create(W, H)
+    try:
+        svgf_theirs = device_ms(lambda: L.refsvgf_run(ref, *ptrs, C.byref(cams[0]), C.byref(sv), out.data_ptr()))
+    finally:
+        L.refsvgf_destroy(ref)
+    rec = {"frame_p50_ms": ours[0], "frame_p99_ms": ours[1], "photon_frame_p50_ms": theirs[0], "photon_frame_p99_ms": theirs[1],
+           "svgf_ms": svgf_ours, "photon_svgf_ms": svgf_theirs}
+    print("REALTIME_VS_PHOTON " + json.dumps(rec))
+    assert svgf_ours < svgf_theirs
