@@ -192,7 +192,9 @@ def systems_sections(r, g, desc, rank):
     - served: a Poisson stream of 400 requests at 40 req/s over the 36-triangle box and the 262K scene
       (resolution / spp / depth drawn as in the serving configuration) through the server, against
       the same stream rendered one request at a time in arrival order; p50/p99 latency from
-      submission to result."""
+      submission to result;
+    - sessions: eight real-time SVGF sessions (1600x900, 1 spp per frame, 120-frame orbits) on host
+      threads; p50/p99 frame time."""
     from photon_b200 import abi, native, serving, workloads
     out = {}
     views = workloads.batch_views(desc, 64, seed=2)
@@ -223,6 +225,10 @@ def systems_sections(r, g, desc, rank):
     rb.close()
     out["served"] = {"workload": "Poisson, 400 requests at 40 req/s, seed 7, scenes: 36-triangle box + 262K terrain",
                      "served": served, "plain": plain, "budget_bytes": 150 << 30}
+    from photon_b200 import sessions
+    out["sessions"] = dict(sessions.run_sessions(desc, 8, 120, 1600, 900),
+                           workload="8 real-time SVGF sessions, 120-frame orbits (0.5 deg/frame) of the 262K scene, 1600x900, 1 spp",
+                           api="pt_render_denoised")
     return out
 
 

@@ -15,14 +15,17 @@ import numpy as np
 from . import abi, native, workloads
 
 
-def run_sessions(desc, n_sessions=8, frames=120, width=1600, height=900, max_depth=12, device=0, warmup=3):
+def run_sessions(desc, n_sessions=8, frames=120, width=1600, height=900, max_depth=12, device=0, warmup=3, tuning=None):
     """Returns {"sessions", "frames", "p50_ms", "p99_ms", "mean_ms", "frames_per_s", ...}; frame time is
-    the wall clock of one pt_render_denoised call (render, G-buffer, SVGF, synchronised)."""
+    the wall clock of one pt_render_denoised call (render, G-buffer, SVGF, synchronised). `tuning`:
+    pt_set_tuning fields applied to every session's renderer."""
     renderers, cams = [], []
     for k in range(n_sessions):
         r = native.Renderer(device)
         r.upload(desc)
         r.resize(width, height)
+        if tuning:
+            r.set_tuning(**tuning)
         renderers.append(r)
         cams.append(workloads.orbit_cameras(desc, frames + warmup, width / height, start_deg=45.0 * k))
     rs = abi.render_settings(width, height, max_depth=max_depth, seed=11)

@@ -4,6 +4,7 @@ the parity bar), and its throughput next to the wavefront's on the 262,144-trian
 depth-12 frame (8-spp launches after a 4-spp warm-up, as `photon bench` runs it)."""
 import ctypes as C
 import json
+import threading
 import os
 import time
 
@@ -123,11 +124,12 @@ def test_batched_views_vs_photon_megakernel(L):
     assert rec["speedup"] > 1.0
 
 
-def test_realtime_sessions_vs_photon(L, torch_cuda=None):
+def test_realtime_sessions_vs_photon(L):
     """Real-time frames (1 spp + G-buffer + SVGF) on an orbit of the 262K scene at 1600x900: one
     session through pt_render_denoised against Photon's GpuRenderer::render_denoised (megakernel +
-    svgf.cu), and SVGF alone, ours against svgf.cu, on identical G-buffers. Frame times are wall clock
-    of the synchronous calls; percentiles over the orbit's frames."""
+    svgf.cu); SVGF alone, ours against svgf.cu, on identical G-buffers; and eight concurrent sessions
+    (host threads) of each. Frame times are wall clock of the synchronous calls; percentiles over the
+    orbit's frames."""
     import torch
     from photon_b200 import workloads
     desc, camf, keep = scenes.scene("terrain")
@@ -186,7 +188,46 @@ def test_realtime_sessions_vs_photon(L, torch_cuda=None):
         svgf_theirs = device_ms(lambda: L.refsvgf_run(ref, *ptrs, C.byref(cams[0]), C.byref(sv), out.data_ptr()))
     finally:
         L.refsvgf_destroy(ref)
+    # Eight concurrent sessions (host threads), 30 frames each, 45 degrees apart on the orbit.
+    from photon_b200 import sessions
+    ours8 = sessions.run_sessions(desc, 8, 30, W, H)
+    lat = [[] for _ in range(8)]
+    gs = []
+    try:
+        for k in range(8):
+            gk = L.refgpu_create()
+            gs.append(gk)
+            assert L.refgpu_upload(gk, ref_scene.h)
+            L.refgpu_resize(gk, W, H)
+        orbits = [workloads.orbit_cameras(desc, 33, W / H, start_deg=45.0 * k) for k in range(8)]
+        barrier = threading.Barrier(9)
+
+        def photon_session(k):
+            cs = orbits[k]
+            for f in range(3):
+                L.refgpu_render_denoised(gs[k], C.byref(cs[f]), C.byref(cs[max(f - 1, 0)]), C.byref(rs), C.byref(sv))
+            barrier.wait()
+            for f in range(3, 33):
+                t0 = time.perf_counter()
+                L.refgpu_render_denoised(gs[k], C.byref(cs[f]), C.byref(cs[f - 1]), C.byref(rs), C.byref(sv))
+                lat[k].append((time.perf_counter() - t0) * 1e3)
+
+        threads = [threading.Thread(target=photon_session, args=(k,)) for k in range(8)]
+        for t in threads:
+            t.start()
+        barrier.wait()
+        t0 = time.perf_counter()
+        for t in threads:
+            t.join()
+        wall = time.perf_counter() - t0
+    finally:
+        for gk in gs:
+            L.refgpu_destroy(gk)
+    all_lat = np.concatenate([np.asarray(x) for x in lat])
     rec = {"frame_p50_ms": ours[0], "frame_p99_ms": ours[1], "photon_frame_p50_ms": theirs[0], "photon_frame_p99_ms": theirs[1],
-           "svgf_ms": svgf_ours, "photon_svgf_ms": svgf_theirs}
+           "svgf_ms": svgf_ours, "photon_svgf_ms": svgf_theirs,
+           "sessions8_p50_ms": ours8["p50_ms"], "sessions8_p99_ms": ours8["p99_ms"], "sessions8_frames_per_s": ours8["frames_per_s"],
+           "photon_sessions8_p50_ms": float(np.percentile(all_lat, 50)), "photon_sessions8_p99_ms": float(np.percentile(all_lat, 99)),
+           "photon_sessions8_frames_per_s": all_lat.size / wall}
     print("REALTIME_VS_PHOTON " + json.dumps(rec))
     assert svgf_ours < svgf_theirs
