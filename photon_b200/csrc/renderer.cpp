@@ -233,6 +233,17 @@ void WavefrontEngine::iterate(int iterations) {
     PTW_CUDA(cudaMemcpyAsync(h_ctr_, ctr_.ptr, sizeof(Counters), cudaMemcpyDeviceToHost, stream_));
 }
 
+void WavefrontEngine::launch(int iterations) {
+    for (int k = 0; k < iterations; k++) PTW_CUDA(wf_iteration(cont_params_, shape_, stream_));
+    kernel_launches += uint64_t(iterations) * kKernelsPerIteration;
+    iteration_launches += uint64_t(iterations);
+}
+
+void WavefrontEngine::set_work_total_async(const unsigned long long* pinned_value) {
+    PTW_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(ctr_.ptr) + offsetof(Counters, work_total), pinned_value, sizeof(unsigned long long),
+                             cudaMemcpyHostToDevice, stream_));
+}
+
 void WavefrontEngine::sync() {
     PTW_CUDA(cudaEventRecord(ev_, stream_));
     PTW_CUDA(cudaEventSynchronize(ev_));
@@ -280,16 +291,17 @@ void Renderer::resize(int w, int h) {
     PTW_CUDA(cudaSetDevice(device_));
     width_ = w;
     height_ = h;
+    // The per-pixel buffers only grow, so a renderer that serves images of several sizes does not
+    // free and allocate (each a device-wide synchronisation) on every size change. The denoiser's
+    // buffers are sized on the first real-time frame.
     size_t n = size_t(w) * size_t(h);
     for (DeviceBuffer<float4>* b : {&accum_, &albedo_, &normal_depth_, &edge_, &motion_, &emission_, &color_, &denoised_buf_}) {
-        b->allocate(n);
-        b->zero(stream_);
+        b->reserve(n);
+        if (n) PTW_CUDA(cudaMemsetAsync(b->ptr, 0, n * sizeof(float4), stream_));
     }
-    heat_.allocate(n);
-    display_.allocate(n);
-    display_.zero(stream_);
-    if (!svgf_) svgf_ = std::make_unique<SvgfDenoiser>(device_, stream_);
-    svgf_->resize(w, h);
+    heat_.reserve(n);
+    display_.reserve(n);
+    if (n) PTW_CUDA(cudaMemsetAsync(display_.ptr, 0, n * sizeof(uint32_t), stream_));
     PTW_CUDA(cudaStreamSynchronize(stream_));
     reset();
 }
@@ -438,6 +450,8 @@ void Renderer::render_denoised(const pt_camera& cam, const pt_camera& prev, cons
     if (!scene_.ready()) throw Error{PT_ERR_NO_SCENE, "render before upload"};
     if (width_ == 0 || height_ == 0) return;
     PTW_CUDA(cudaSetDevice(device_));
+    if (!svgf_) svgf_ = std::make_unique<SvgfDenoiser>(device_, stream_);
+    svgf_->resize(width_, height_);
     if (!denoised_) {
         samples_ = 0;
         svgf_->reset();
@@ -496,7 +510,9 @@ void Renderer::display(const pt_render_settings& rs, int mode, uint32_t* target)
     p.max_depth = scene_.extent();
     p.heat_scale = 1.0f / 160.0f;
     p.denoised = denoised_ ? 1 : 0;
-    const float4* variance = svgf_ ? reinterpret_cast<const float4*>(svgf_->variance()) : nullptr;
+    const float4* variance = svgf_ && svgf_->width() == width_ && svgf_->height() == height_
+                                 ? reinterpret_cast<const float4*>(svgf_->variance())
+                                 : nullptr;
     PTW_CUDA(wf_display(p, accum_.ptr, denoised_buf_.ptr, albedo_.ptr, normal_depth_.ptr, variance, heat_.ptr,
                         target ? target : display_.ptr, stream_));
     PTW_CUDA(cudaStreamSynchronize(stream_));

@@ -53,6 +53,12 @@ public:
     void iterate(int iterations);           // launches iterations and copies the counters back
     const Counters& counters() const { return *h_ctr_; }  // valid after sync()
     void sync();
+    // Pipelined continuous mode: launches `iterations` bounce iterations and nothing else; the caller
+    // copies the counters (device_counters) itself and raises work_total with a stream-ordered copy
+    // from its own staging memory (set_work_total_async).
+    void launch(int iterations);
+    Counters* device_counters() const { return ctr_.ptr; }
+    void set_work_total_async(const unsigned long long* pinned_value);
 
     const Counters& last() const { return last_; }
 

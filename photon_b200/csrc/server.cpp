@@ -1,12 +1,17 @@
 // The request server (continuous batching over resident scenes).
 //
 // A server thread owns one device stream and one wavefront engine in continuous mode. Requests are
-// admitted in arrival order while they fit the device-memory budget: each admitted request becomes
-// a view (camera, size, spp, seed, scene slot) whose work range is appended to the running
-// wavefront, so its paths share the path pool with every other request in flight, whatever their
-// scene, resolution or spp. Between graph-sized batches of bounce iterations the thread reads the
-// per-view finished-path counters; a request whose paths have all finished is summed in sample
-// order (so its image is the same alone or in any mix), copied to the host and released.
+// admitted in arrival order while they fit the device-memory budget; an admitted request's paths are
+// handed to the running wavefront in chunks, so they share the path pool with every other request
+// in flight, whatever their scene, resolution or spp. The thread keeps about one pool's worth of
+// handed-over paths ahead of generation and fills it shortest-remaining-request first, so a small
+// request that arrives behind a large one waits for one chunk, not for the whole large image.
+// Each chunk is a view (camera, size, spp, seed, scene slot) over a range of the image's work items;
+// all chunks of a request count into one finished-path counter. Between batches of bounce
+// iterations the thread reads the counters; a request whose paths have all finished is summed in
+// sample order (so its image is the same alone or in any mix), copied to the host and released.
+// Request buffers come from a private stream-ordered memory pool, so admissions and releases never
+// synchronise the device.
 // The device never waits on anything: kernels claim work with atomics and return, so a stalled
 // request cannot hang the GPU; host waits are all bounded.
 #include "server.h"
@@ -19,7 +24,7 @@ namespace ptw {
 
 namespace {
 constexpr int kMaxScenes = 256;
-constexpr int kItersPerCheck = 2;
+constexpr uint64_t kChunkPaths = uint64_t(1) << 20;  // paths per chunk handed to the wavefront
 }  // namespace
 
 Server::Server(const pt_server_config& cfg) : cfg_(cfg), device_(cfg.device) {
@@ -36,6 +41,21 @@ Server::Server(const pt_server_config& cfg) : cfg_(cfg), device_(cfg.device) {
     d_views_.allocate(1024);
     d_done_.allocate(1024);
     d_done_.zero(stream_);
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device_;
+    PTW_CUDA(cudaMemPoolCreate(&mem_pool_, &props));
+    uint64_t keep = ~uint64_t(0);  // freed request buffers stay in the pool for the next admissions
+    PTW_CUDA(cudaMemPoolSetAttribute(mem_pool_, cudaMemPoolAttrReleaseThreshold, &keep));
+    PTW_CUDA(cudaStreamCreateWithFlags(&fin_stream_, cudaStreamNonBlocking));
+    for (Batch& b : batch_) {
+        PTW_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&b.ctr), sizeof(Counters), cudaHostAllocDefault));
+        PTW_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&b.work_total), sizeof(unsigned long long), cudaHostAllocDefault));
+        PTW_CUDA(cudaEventCreate(&b.ev));
+        PTW_CUDA(cudaEventCreate(&b.ev_start));
+        std::memset(b.ctr, 0, sizeof(Counters));
+    }
     PTW_CUDA(cudaStreamSynchronize(stream_));
     st_.budget_bytes = cfg.budget_bytes;
     if (cfg_.budget_bytes && pool_bytes_ > cfg_.budget_bytes) throw Error{PT_ERR_BUDGET, "the path pool alone exceeds the budget"};
@@ -51,9 +71,25 @@ Server::~Server() {
     if (thread_.joinable()) thread_.join();
     cudaSetDevice(device_);
     cudaStreamSynchronize(stream_);
+    cudaStreamSynchronize(fin_stream_);
+    for (auto& kv : requests_) release_buffers(*kv.second, stream_);
+    for (Finishing& f : finishing_) cudaEventDestroy(f.ev);
+    for (auto& kv : requests_)
+        if (kv.second->result) cudaFreeHost(kv.second->result);
+    cudaStreamSynchronize(stream_);
+    for (Batch& b : batch_) {
+        cudaFreeHost(b.ctr);
+        cudaFreeHost(b.work_total);
+        if (b.done) cudaFreeHost(b.done);
+        cudaEventDestroy(b.ev);
+        cudaEventDestroy(b.ev_start);
+    }
+    for (auto& kv : pinned_free_) cudaFreeHost(kv.second);
     requests_.clear();
     engine_.reset();
     scenes_.clear();
+    if (mem_pool_) cudaMemPoolDestroy(mem_pool_);
+    cudaStreamDestroy(fin_stream_);
     cudaStreamDestroy(stream_);
 }
 
@@ -158,10 +194,12 @@ void Server::fetch(uint64_t id, float* rgb, size_t n, pt_request_stats* st) {
         st->state = r.state;
     }
     if (r.state == PT_REQ_DONE && rgb) {
-        if (n < r.result.size()) throw Error{PT_ERR_INVALID, "fetch: buffer too small"};
-        std::memcpy(rgb, r.result.data(), r.result.size() * sizeof(float));
+        if (n < 3 * size_t(r.req.width) * size_t(r.req.height)) throw Error{PT_ERR_INVALID, "fetch: buffer too small"};
+        std::memcpy(rgb, r.result, 3 * size_t(r.req.width) * size_t(r.req.height) * sizeof(float));
     }
     int state = r.state;
+    pinned_release(r.result, r.result_bytes);
+    r.result = nullptr;
     requests_.erase(it);
     if (state == PT_REQ_CANCELLED) throw Error{PT_ERR_CANCELLED, "request cancelled"};
 }
@@ -205,7 +243,46 @@ void Server::upload_scene_table() {
     scenes_dirty_ = false;
 }
 
-// Called with the lock held: allocates the request's buffers and appends its view.
+void Server::release_buffers(Request& r, cudaStream_t s) {
+    if (r.sample_out) cudaFreeAsync(r.sample_out, s);
+    if (r.accum) cudaFreeAsync(r.accum, s);
+    r.sample_out = r.accum = nullptr;
+}
+
+// Pinned host staging for finished images (the result a fetch copies out), reused across requests.
+// Blocks come in power-of-two sizes (at least 64 KiB) and are kept by size; a request takes the
+// smallest one that fits. Pinning is slow, so after a warm-up the pool serves every request.
+static size_t pinned_class(size_t bytes) {
+    size_t c = size_t(1) << 16;
+    while (c < bytes) c <<= 1;
+    return c;
+}
+
+float* Server::pinned_acquire(size_t bytes) {
+    bytes = pinned_class(bytes);
+    {
+        std::lock_guard<std::mutex> g(pinned_mu_);
+        auto it = pinned_free_.lower_bound(bytes);
+        if (it != pinned_free_.end()) {
+            float* p = it->second;
+            pinned_free_.erase(it);
+            return p;
+        }
+    }
+    float* p = nullptr;
+    PTW_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&p), bytes, cudaHostAllocDefault));
+    return p;
+}
+
+void Server::pinned_release(float* p, size_t bytes) {
+    if (!p) return;
+    bytes = pinned_class(bytes);
+    std::lock_guard<std::mutex> g(pinned_mu_);
+    pinned_free_.emplace(bytes, p);
+}
+
+// Called with the lock held: allocates the request's buffers and its finished-path counter. Its work
+// is handed to the wavefront later, chunk by chunk (append_chunks).
 bool Server::try_admit(Request& r) {
     if (cfg_.max_active > 0 && int(active_.size()) >= cfg_.max_active) return false;
     if (cfg_.budget_bytes && bytes_in_use_ + r.bytes + pool_bytes_ + scene_bytes_ > cfg_.budget_bytes) return false;
@@ -215,34 +292,37 @@ bool Server::try_admit(Request& r) {
             inject_failures_--;
             throw Error{PT_ERR_ALLOC, "injected allocation failure"};
         }
-        r.sample_out.allocate(npix * size_t(r.req.spp));
-        r.accum.allocate(npix);
-        r.accum.zero(stream_);
+        PTW_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r.sample_out), npix * size_t(r.req.spp) * sizeof(float4), mem_pool_,
+                                         stream_));
+        PTW_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r.accum), npix * sizeof(float4), mem_pool_, stream_));
+        PTW_CUDA(cudaMemsetAsync(r.accum, 0, npix * sizeof(float4), stream_));
     } catch (const Error& e) {
-        r.sample_out.release();
-        r.accum.release();
+        cudaGetLastError();
+        release_buffers(r, stream_);
         r.state = PT_REQ_FAILED;
         r.error = e.message;
         r.done_s = now();
         cv_done_.notify_all();
         return true;  // consumed (failed), not retried
     }
-    // Grow the view table (and the finished-path counters) by doubling.
-    if (views_.size() + 1 > d_views_.count) {
-        size_t cap = d_views_.count * 2;
-        DeviceBuffer<DevView> nv;
-        nv.allocate(cap);
+    // Grow the finished-path counters by doubling.
+    if (size_t(done_slots_) + 1 > d_done_.count) {
         DeviceBuffer<unsigned long long> nd;
-        nd.allocate(cap);
+        nd.allocate(d_done_.count * 2);
         nd.zero(stream_);
         PTW_CUDA(cudaMemcpyAsync(nd.ptr, d_done_.ptr, d_done_.bytes(), cudaMemcpyDeviceToDevice, stream_));
         PTW_CUDA(cudaStreamSynchronize(stream_));
-        d_views_ = std::move(nv);
         d_done_ = std::move(nd);
-        for (size_t k = 0; k < views_.size(); k++) views_[k].done_counter = d_done_.ptr + k;
+        for (auto& kv : requests_) {
+            Request& q = *kv.second;
+            if (q.done_slot < 0) continue;
+            q.tmpl.done_counter = d_done_.ptr + q.done_slot;
+            for (int vi : q.views) views_[size_t(vi)].done_counter = q.tmpl.done_counter;
+        }
         views_uploaded_ = 0;  // re-upload everything
     }
-    DevView v;
+    r.done_slot = done_slots_++;
+    DevView& v = r.tmpl;
     std::memset(&v, 0, sizeof(v));
     std::memcpy(v.cam, &r.req.camera, sizeof(v.cam));
     v.width = r.req.width;
@@ -255,14 +335,9 @@ bool Server::try_admit(Request& r) {
     v.rr_depth = r.req.path.rr_depth;
     v.nee = r.req.path.nee;
     v.clamp = r.req.path.clamp;
-    v.work_begin = work_total_;
-    v.work_count = r.work;
-    v.sample_out = r.sample_out.ptr;
-    v.accum = r.accum.ptr;
-    v.done_counter = d_done_.ptr + views_.size();
-    r.view = int(views_.size());
-    views_.push_back(v);
-    work_total_ += r.work;
+    v.sample_out = r.sample_out;
+    v.accum = r.accum;
+    v.done_counter = d_done_.ptr + r.done_slot;
     bytes_in_use_ += r.bytes;
     r.state = PT_REQ_RUNNING;
     r.admit_s = now();
@@ -270,20 +345,35 @@ bool Server::try_admit(Request& r) {
     return true;
 }
 
-// Sums a finished request's samples in order and copies its image to the host (lock released).
-void Server::finish(Request& r) {
-    const DevView& v = views_[size_t(r.view)];
-    PTW_CUDA(wf_accumulate(d_views_.ptr + r.view, v, 1, 1, stream_));
-    size_t npix = size_t(r.req.width) * size_t(r.req.height);
-    std::vector<float4> raw(npix);
-    PTW_CUDA(cudaMemcpyAsync(raw.data(), r.accum.ptr, npix * sizeof(float4), cudaMemcpyDeviceToHost, stream_));
-    PTW_CUDA(cudaStreamSynchronize(stream_));
-    r.result.resize(3 * npix);
-    float inv = 1.0f / float(r.req.spp);
-    for (size_t i = 0; i < npix; i++) {
-        r.result[3 * i] = raw[i].x * inv;
-        r.result[3 * i + 1] = raw[i].y * inv;
-        r.result[3 * i + 2] = raw[i].z * inv;
+// Called with the lock held: hands chunks of the running requests' work to the wavefront, shortest
+// remaining request first, until about one path pool's worth waits ahead of generation.
+void Server::append_chunks() {
+    const uint64_t generated = generated_;
+    // Two batches run between a counter read and the next append: keep both supplied.
+    const uint64_t target = (2 * uint64_t(iters_per_batch_) + 1) * uint64_t(engine_->tuning().path_capacity);
+    while (work_total_ < generated + target) {
+        Request* best = nullptr;
+        for (uint64_t id : active_) {
+            Request& r = *requests_[id];
+            if (r.cancel || r.appended >= r.work) continue;
+            if (!best || r.work - r.appended < best->work - best->appended) best = &r;
+        }
+        if (!best) break;
+        const uint64_t n = std::min(best->work - best->appended, kChunkPaths);
+        if (views_.size() + 1 > d_views_.count) {
+            DeviceBuffer<DevView> nv;
+            nv.allocate(d_views_.count * 2);
+            d_views_ = std::move(nv);
+            views_uploaded_ = 0;  // re-upload everything
+        }
+        DevView v = best->tmpl;
+        v.work_begin = work_total_;
+        v.work_count = n;
+        v.local_base = best->appended;
+        best->views.push_back(int(views_.size()));
+        views_.push_back(v);
+        best->appended += n;
+        work_total_ += n;
     }
 }
 
@@ -291,15 +381,19 @@ void Server::loop() {
     cudaSetDevice(device_);
     std::unique_lock<std::mutex> lk(mu_);
     double busy_since = -1;
+    int cur = 0;
     while (!stop_) {
         try {
-            // Admission in arrival order while the budget allows.
+            // Admission in arrival order while the budget allows, then chunks of work.
             while (!queue_.empty()) {
                 Request& r = *requests_[queue_.front()];
                 if (!try_admit(r)) break;
                 queue_.pop_front();
             }
+            append_chunks();
             if (scenes_dirty_) upload_scene_table();
+            Batch& B = batch_[cur];
+            Batch& P = batch_[cur ^ 1];
             if (views_uploaded_ < views_.size()) {
                 PTW_CUDA(cudaMemcpyAsync(d_views_.ptr + views_uploaded_, views_.data() + views_uploaded_,
                                          (views_.size() - views_uploaded_) * sizeof(DevView), cudaMemcpyHostToDevice, stream_));
@@ -309,19 +403,24 @@ void Server::loop() {
                     engine_started_ = true;
                 }
                 engine_->set_views(d_views_.ptr, int(views_.size()));
-                engine_->append_work(work_total_);
+                *B.work_total = work_total_;  // B's previous batch has completed: its staging is free
+                engine_->set_work_total_async(B.work_total);
             }
-            // Cancelled running requests: their remaining paths end at their first vertex.
+            // Cancelled running requests: no further chunks, and the paths of those handed over end at
+            // their first vertex.
             for (uint64_t id : active_) {
                 Request& r = *requests_[id];
-                if (r.cancel && views_[size_t(r.view)].max_depth != 0) {
-                    views_[size_t(r.view)].max_depth = 0;
-                    PTW_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(d_views_.ptr + r.view) + offsetof(DevView, max_depth),
-                                             &views_[size_t(r.view)].max_depth, sizeof(int), cudaMemcpyHostToDevice, stream_));
+                if (!r.cancel) continue;
+                for (int vi : r.views) {
+                    if (views_[size_t(vi)].max_depth == 0) continue;
+                    views_[size_t(vi)].max_depth = 0;
+                    PTW_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(d_views_.ptr + vi) + offsetof(DevView, max_depth),
+                                             &views_[size_t(vi)].max_depth, sizeof(int), cudaMemcpyHostToDevice, stream_));
                     PTW_CUDA(cudaStreamSynchronize(stream_));
                 }
             }
-            if (active_.empty()) {
+            const bool launch = !active_.empty();
+            if (!launch && !P.in_flight && finishing_.empty()) {
                 if (busy_since >= 0) {
                     st_.busy_seconds += now() - busy_since;
                     busy_since = -1;
@@ -330,44 +429,133 @@ void Server::loop() {
                 continue;
             }
             if (busy_since < 0) busy_since = now();
-            // A batch of bounce iterations with the lock released.
-            std::vector<Request*> active;
-            for (uint64_t id : active_) active.push_back(requests_[id].get());
+            // Snapshot of this batch's requests and their counter range.
+            B.reqs.clear();
+            B.need.clear();
+            size_t lo = size_t(done_slots_), hi = 0;
+            for (uint64_t id : active_) {
+                Request* r = requests_[id].get();
+                B.reqs.push_back(r);
+                B.need.push_back(r->cancel ? r->appended : r->work);
+                lo = std::min(lo, size_t(r->done_slot));
+                hi = std::max(hi, size_t(r->done_slot) + 1);
+            }
+            if (hi < lo) hi = lo;
+            B.lo = lo;
+            B.n = hi - lo;
+            if (B.n > B.done_cap) {
+                if (B.done) PTW_CUDA(cudaFreeHost(B.done));
+                B.done_cap = std::max<size_t>(B.n * 2, 1024);
+                PTW_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&B.done), B.done_cap * sizeof(unsigned long long), cudaHostAllocDefault));
+            }
+            const unsigned long long* d_done = d_done_.ptr;
             lk.unlock();
-            engine_->iterate(kItersPerCheck);
-            engine_->sync();
-            if (h_done_.size() < views_.size()) h_done_.resize(views_.size());
-            size_t lo = views_.size(), hi = 0;
-            for (Request* r : active) {
-                size_t vi = size_t(r->view);
-                lo = std::min(lo, vi);
-                hi = std::max(hi, vi + 1);
+
+            // Launch this batch, then read the previous one's results while it runs.
+            if (launch) {
+                B.iterations = iters_per_batch_;
+                PTW_CUDA(cudaEventRecord(B.ev_start, stream_));
+                engine_->launch(B.iterations);
+                PTW_CUDA(cudaMemcpyAsync(B.ctr, engine_->device_counters(), sizeof(Counters), cudaMemcpyDeviceToHost, stream_));
+                if (B.n)
+                    PTW_CUDA(cudaMemcpyAsync(B.done, d_done + B.lo, B.n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_));
+                PTW_CUDA(cudaEventRecord(B.ev, stream_));
+                B.in_flight = true;
             }
-            PTW_CUDA(cudaMemcpyAsync(h_done_.data() + lo, d_done_.ptr + lo, (hi - lo) * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_));
-            PTW_CUDA(cudaStreamSynchronize(stream_));
-            std::vector<Request*> finished;
-            for (Request* r : active)
-                if (h_done_[size_t(r->view)] >= r->work) finished.push_back(r);
-            for (Request* r : finished)
-                if (!r->cancel) finish(*r);
-            lk.lock();
-            st_.bounce_iterations = engine_->counters().iterations;
-            for (Request* r : finished) {
-                r->state = r->cancel ? PT_REQ_CANCELLED : PT_REQ_DONE;
-                r->done_s = now();
-                if (r->cancel) st_.cancelled++;
-                else {
-                    st_.completed++;
-                    st_.samples_done += r->work;
+            std::vector<Request*> finished, cancelled;
+            if (P.in_flight) {
+                PTW_CUDA(cudaEventSynchronize(P.ev));
+                P.in_flight = false;
+                generated_ = P.ctr->work_next;
+                iterations_ = P.ctr->iterations;
+                // Aim for batches of about a millisecond of device time: long enough that the host's
+                // turn between batches stays hidden, short enough that finished requests and new
+                // arrivals are seen soon.
+                float ms = 0.0f;
+                if (cudaEventElapsedTime(&ms, P.ev_start, P.ev) == cudaSuccess && ms > 0.0f) {
+                    double want = double(P.iterations) * (1.0 / double(ms));
+                    iters_per_batch_ = std::max(1, std::min(16, int(want + 0.5)));
                 }
-                bytes_in_use_ -= r->bytes;
-                r->sample_out.release();
-                r->accum.release();
-                active_.erase(std::remove(active_.begin(), active_.end(), r->id), active_.end());
+                for (size_t k = 0; k < P.reqs.size(); k++) {
+                    Request* r = P.reqs[k];
+                    if (r->finishing || P.done[size_t(r->done_slot) - P.lo] < P.need[k]) continue;
+                    r->finishing = true;  // the batch launched meanwhile also lists it: finish once
+                    (r->cancel ? cancelled : finished).push_back(r);
+                }
+                // Sum each finished request's samples in order and copy its image out, on the second
+                // stream after the batch that finished it; release its buffers behind the copy.
+                for (Request* r : finished) {
+                    const uint32_t npix = uint32_t(r->req.width) * uint32_t(r->req.height);
+                    const int first = r->views.front();  // carries the whole image's spp and buffers
+                    PTW_CUDA(cudaStreamWaitEvent(fin_stream_, P.ev, 0));
+                    PTW_CUDA(wf_accumulate(d_views_.ptr + first, views_[size_t(first)], 1, 1, fin_stream_));
+                    // The averaged rgb image goes into the (no longer needed) sample buffer, then to
+                    // pinned host memory that fetch copies from.
+                    float* rgb = reinterpret_cast<float*>(r->sample_out);
+                    PTW_CUDA(wf_resolve(r->accum, npix, 1.0f / float(r->req.spp), rgb, fin_stream_));
+                    r->result_bytes = size_t(npix) * 3 * sizeof(float);
+                    r->result = pinned_acquire(r->result_bytes);
+                    PTW_CUDA(cudaMemcpyAsync(r->result, rgb, r->result_bytes, cudaMemcpyDeviceToHost, fin_stream_));
+                    release_buffers(*r, fin_stream_);
+                    Finishing f{r, nullptr};
+                    PTW_CUDA(cudaEventCreateWithFlags(&f.ev, cudaEventDisableTiming));
+                    PTW_CUDA(cudaEventRecord(f.ev, fin_stream_));
+                    finishing_.push_back(f);
+                }
+                for (Request* r : cancelled) release_buffers(*r, stream_);
             }
-            if (!finished.empty()) cv_done_.notify_all();
+            // Images whose copy has landed: normalise by the sample count. With nothing else to do,
+            // wait for the oldest copy instead of polling.
+            if (!launch && !finishing_.empty() && finished.empty()) PTW_CUDA(cudaEventSynchronize(finishing_.front().ev));
+            std::vector<Request*> done;
+            for (size_t k = 0; k < finishing_.size();) {
+                Finishing& f = finishing_[k];
+                cudaError_t q = cudaEventQuery(f.ev);
+                if (q == cudaErrorNotReady) {
+                    k++;
+                    continue;
+                }
+                PTW_CUDA(q);
+                cudaEventDestroy(f.ev);
+                done.push_back(f.r);
+                finishing_.erase(finishing_.begin() + std::ptrdiff_t(k));
+            }
+            lk.lock();
+            st_.bounce_iterations = iterations_;
+            // A request leaves the active list once its image is being finished (the next batches no
+            // longer carry it); its memory counts against the budget until the copy has landed.
+            auto deactivate = [&](Request* r) { active_.erase(std::remove(active_.begin(), active_.end(), r->id), active_.end()); };
+            for (Request* r : finished) deactivate(r);
+            for (Request* r : cancelled) {
+                deactivate(r);
+                r->state = PT_REQ_CANCELLED;
+                r->done_s = now();
+                bytes_in_use_ -= r->bytes;
+                st_.cancelled++;
+            }
+            for (Request* r : done) {
+                r->state = PT_REQ_DONE;
+                r->done_s = now();
+                bytes_in_use_ -= r->bytes;
+                st_.completed++;
+                st_.samples_done += r->work;
+            }
+            if (!done.empty() || !cancelled.empty()) cv_done_.notify_all();
+            cur ^= 1;
         } catch (const Error& e) {
             if (!lk.owns_lock()) lk.lock();
+            cudaStreamSynchronize(stream_);
+            cudaStreamSynchronize(fin_stream_);
+            cudaGetLastError();
+            for (Batch& b : batch_) b.in_flight = false;
+            for (Finishing& f : finishing_) {
+                cudaEventDestroy(f.ev);
+                f.r->state = PT_REQ_FAILED;
+                f.r->error = e.message;
+                f.r->done_s = now();
+                bytes_in_use_ -= f.r->bytes;
+            }
+            finishing_.clear();
             // A device failure fails every running request; the server keeps its handle valid.
             for (uint64_t id : active_) {
                 Request& r = *requests_[id];
@@ -375,6 +563,7 @@ void Server::loop() {
                 r.error = e.message;
                 r.done_s = now();
                 bytes_in_use_ -= r.bytes;
+                release_buffers(r, stream_);
             }
             active_.clear();
             cv_done_.notify_all();

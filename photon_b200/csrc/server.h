@@ -2,6 +2,7 @@
 // wavefront, admission by device-memory budget.
 #pragma once
 
+#include <atomic>
 #include <condition_variable>
 #include <deque>
 #include <map>
@@ -39,18 +40,27 @@ private:
         double submit_s = 0, admit_s = 0, done_s = 0;
         uint64_t work = 0;
         size_t bytes = 0;
-        int view = -1;          // index in the view table once admitted
-        bool cancel = false;
+        uint64_t appended = 0;  // paths handed to the wavefront so far
+        std::vector<int> views; // its chunks in the view table (the first also serves the accumulation)
+        int done_slot = -1;     // its finished-path counter
+        DevView tmpl{};         // the view of the whole image; chunks differ in work range only
+        std::atomic<bool> cancel{false};
+        bool finishing = false;  // its image is being summed and copied out
         std::string error;
-        DeviceBuffer<float4> sample_out, accum;
-        std::vector<float> result;  // rgb, filled when done
+        float4* sample_out = nullptr;  // stream-ordered allocations from the server's memory pool
+        float4* accum = nullptr;
+        float* result = nullptr;  // rgb (pinned, from the server's staging pool), filled when done
+        size_t result_bytes = 0;
     };
 
     void loop();
     double now() const;
     size_t request_bytes(const pt_request& r) const;
     bool try_admit(Request& r);
-    void finish(Request& r);
+    void append_chunks();
+    void release_buffers(Request& r, cudaStream_t s);
+    float* pinned_acquire(size_t bytes);
+    void pinned_release(float* p, size_t bytes);
     void upload_scene_table();
 
     pt_server_config cfg_;
@@ -73,11 +83,39 @@ private:
     std::vector<uint64_t> active_;
     uint64_t next_id_ = 1;
 
-    // The view table grows by one entry per admitted request; work ranges are contiguous.
+    // The view table grows by one entry per appended chunk; work ranges are contiguous.
     std::vector<DevView> views_;
     DeviceBuffer<DevView> d_views_;
-    DeviceBuffer<unsigned long long> d_done_;
+    DeviceBuffer<unsigned long long> d_done_;   // one finished-path counter per admitted request
     std::vector<unsigned long long> h_done_;
+    int done_slots_ = 0;
+    cudaMemPool_t mem_pool_ = nullptr;
+    // Pipelining: while the device runs one batch of bounce iterations, the host reads the counters
+    // of the previous one (pinned copies, one staging set per batch) and finishes requests on a
+    // second stream.
+    struct Batch {
+        Counters* ctr = nullptr;                 // pinned
+        unsigned long long* done = nullptr;      // pinned, finished-path counters [lo, lo + n)
+        size_t done_cap = 0, lo = 0, n = 0;
+        unsigned long long* work_total = nullptr;  // pinned staging of the work total
+        std::vector<Request*> reqs;              // active requests when the batch was launched
+        std::vector<uint64_t> need;              // their paths to finish (all, or those handed over if cancelled)
+        cudaEvent_t ev = nullptr, ev_start = nullptr;
+        int iterations = 0;
+        bool in_flight = false;
+    };
+    Batch batch_[2];
+    struct Finishing {
+        Request* r;
+        cudaEvent_t ev;  // its image has landed in r->result
+    };
+    std::vector<Finishing> finishing_;
+    std::mutex pinned_mu_;
+    std::multimap<size_t, float*> pinned_free_;
+    int iters_per_batch_ = 2;  // adapted so that a batch keeps the device busy for about a millisecond
+    cudaStream_t fin_stream_ = nullptr;
+    uint64_t generated_ = 0;       // work items generated, as of the last completed batch
+    uint64_t iterations_ = 0;
     size_t views_uploaded_ = 0;
     uint64_t work_total_ = 0;
     size_t bytes_in_use_ = 0;

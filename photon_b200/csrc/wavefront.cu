@@ -111,8 +111,10 @@ __device__ __forceinline__ int find_view(const DevView* views, int n, unsigned l
 }
 
 // ---- setup ------------------------------------------------------------------------------------------
-__global__ void k_setup(Counters* c, uint32_t capacity, uint32_t tail_paths) {
+__global__ void k_setup(const __grid_constant__ WfParams P) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    Counters* c = P.ctr;
+    const uint32_t capacity = P.pb.capacity, tail_paths = P.tail_paths;
     uint32_t p = c->parity ^ 1u;
     c->parity = p;
     uint32_t cnt = c->count[p];
@@ -122,6 +124,11 @@ __global__ void k_setup(Counters* c, uint32_t capacity, uint32_t tail_paths) {
     c->gen_base = cnt;
     c->gen_n = n;
     c->work_base = c->work_next;
+    // The views are in work order and generation only moves forward: skip those already generated,
+    // so that the generate step's search covers the few views ahead (a server appends views for ever).
+    uint32_t gv = c->gen_view;
+    while (int(gv) + 1 < P.num_views && P.views[gv + 1].work_begin <= c->work_base) gv++;
+    c->gen_view = gv;
     c->work_next += n;
     c->count[p] = cnt + n;
     c->count[p ^ 1u] = 0;
@@ -144,9 +151,10 @@ __global__ void __launch_bounds__(256) k_generate(const __grid_constant__ WfPara
         uint32_t k = k0 + lane_id();
         if (k >= n) continue;
         unsigned long long wg = wb + k;
-        int vi = find_view(P.views, P.num_views, wg);
+        const int v0 = int(c->gen_view);
+        int vi = v0 + find_view(P.views + v0, P.num_views - v0, wg);
         const DevView& v = P.views[vi];
-        uint32_t local = uint32_t(wg - v.work_begin);
+        uint32_t local = uint32_t(v.local_base + (wg - v.work_begin));
         uint32_t npix = uint32_t(v.width) * uint32_t(v.height);
         uint32_t s = local / npix, q = local - s * npix;
         int x, y;
@@ -882,7 +890,7 @@ cudaError_t wf_iteration(const WfParams& p, const LaunchShape& ls, cudaStream_t 
         if (ev) cudaEventRecordWithFlags(ev[k], stream, flags);
     };
     mark(0);
-    k_setup<<<1, 32, 0, stream>>>(p.ctr, p.pb.capacity, p.tail_paths);
+    k_setup<<<1, 32, 0, stream>>>(p);
     mark(1);
     k_generate<<<ls.gen_grid, ls.gen_block, 0, stream>>>(p);
     mark(2);
@@ -898,6 +906,21 @@ cudaError_t wf_iteration(const WfParams& p, const LaunchShape& ls, cudaStream_t 
         k_sort_finish<<<1, 32, 0, stream>>>(p.ctr);
     }
     mark(5);
+    return cudaGetLastError();
+}
+
+__global__ void k_resolve(const float4* __restrict__ accum, uint32_t n, float scale, float* __restrict__ rgb) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 a = accum[i];
+    rgb[3 * size_t(i)] = a.x * scale;
+    rgb[3 * size_t(i) + 1] = a.y * scale;
+    rgb[3 * size_t(i) + 2] = a.z * scale;
+}
+
+cudaError_t wf_resolve(const float4* accum, uint32_t n, float scale, float* rgb, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    k_resolve<<<(n + 255) / 256, 256, 0, stream>>>(accum, n, scale, rgb);
     return cudaGetLastError();
 }
 

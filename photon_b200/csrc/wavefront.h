@@ -21,6 +21,7 @@ struct DevView {
     int gbuffer;              // 1: sample 0 writes the first-hit G-buffer
     int realtime;             // 1: the accumulate step also writes `color` (sample 0)
     unsigned long long work_begin, work_count;
+    unsigned long long local_base;   // index of the view's first work item within its image's samples
     float4* sample_out;       // work_count radiance values, indexed by (sample * pixels + tile slot)
     float4* accum;            // rgb sum + luminance^2 sum per pixel
     float4* acc_pass;         // running per-call sum across passes (may be null for single-pass calls)
@@ -47,6 +48,7 @@ struct Counters {
     uint32_t fetch[6];               // work-claim counters: generate, trace, shade, shadow, sort scatter, tail
     uint32_t overflow;
     uint32_t tail;                   // 1: this iteration finishes every queued path in k_tail
+    uint32_t gen_view;               // first view whose work is not all generated (views are in work order)
     uint32_t iterations;
     unsigned long long work_base, work_next, work_total;
     unsigned long long rays, shadow_rays, paths_done;
@@ -107,6 +109,8 @@ cudaError_t wf_iteration(const WfParams& p, const LaunchShape& ls, cudaStream_t 
 constexpr int kKernelsPerIteration = 5;
 // Sums the samples of every pixel of a view in sample order (after a pass).
 cudaError_t wf_accumulate(const DevView* d_view, const DevView& h_view, int first_pass, int last_pass, cudaStream_t stream);
+// rgb[3 i + c] = accum[i].c * scale for n pixels (a finished image, averaged over its samples).
+cudaError_t wf_resolve(const float4* accum, uint32_t n, float scale, float* rgb, cudaStream_t stream);
 
 // Probes (same device functions as the wavefront).
 cudaError_t wf_trace_primary(const DevScene* scene, const float* cam16, int w, int h, uint32_t frame, uint32_t seed,

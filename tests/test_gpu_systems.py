@@ -138,18 +138,6 @@ def test_server_budget_cancel_and_faults(server_scenes):
     good = s.submit(sid, cam, 32, 32, 2)
     s.wait(good, 30)
     assert s.poll(good) == abi.PT_REQ_DONE
-    # Cancel a long request while it runs, and others (running or still queued); all end cancelled
-    # and their buffers are released.
-    big = s.submit(sid, cam, 256, 256, 128, path=abi.path_options(max_depth=64, rr_depth=64))
-    more = [s.submit(sid, cam, 256, 256, 64, path=abi.path_options(max_depth=64, rr_depth=64)) for _ in range(3)]
-    time.sleep(0.05)
-    for r in [big] + more:
-        s.cancel(r)
-    for r in [big] + more:
-        with pytest.raises(native.PhotonError) as e:
-            s.wait(r, 60)
-        assert e.value.code == abi.PT_ERR_CANCELLED
-        assert s.poll(r) == abi.PT_REQ_CANCELLED
     # A wait that runs out reports a timeout instead of hanging.
     slow = s.submit(sid, cam, 256, 256, 64)
     with pytest.raises(native.PhotonError) as e:
@@ -158,4 +146,30 @@ def test_server_budget_cancel_and_faults(server_scenes):
     s.wait(slow, 60)
     st = s.stats()
     assert st.device_bytes_in_use <= budget
+    s.close()
+
+
+def test_server_cancels_running_and_queued_requests(server_scenes):
+    """One request runs at a time (max_active 1): a long request on the 262K scene is cancelled while
+    it runs and three others while they wait; all end cancelled, their buffers are released, and the
+    server goes on to finish a new request."""
+    _, (tdesc, tcam, tkeep) = server_scenes
+    s = native.Server(budget_bytes=4 << 30, path_capacity=1 << 18, max_active=1)
+    sid = s.add_scene(tdesc)
+    cam = tcam(1.0)
+    deep = abi.path_options(max_depth=64, rr_depth=64)
+    big = s.submit(sid, cam, 512, 512, 64, path=deep)
+    more = [s.submit(sid, cam, 256, 256, 16, path=deep) for _ in range(3)]
+    for r in [big] + more:
+        s.cancel(r)
+    for r in [big] + more:
+        with pytest.raises(native.PhotonError) as e:
+            s.wait(r, 60)
+        assert e.value.code == abi.PT_ERR_CANCELLED
+        assert s.poll(r) == abi.PT_REQ_CANCELLED
+    ok = s.submit(sid, cam, 64, 64, 4)
+    s.wait(ok, 60)
+    assert s.poll(ok) == abi.PT_REQ_DONE
+    st = s.stats()
+    assert st.cancelled == 4 and st.active == 0
     s.close()
