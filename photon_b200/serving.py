@@ -63,3 +63,65 @@ def run_plain(renderers, stream):
         samples += r["w"] * r["h"] * r["spp"]
     makespan = (time.perf_counter() - t0) - stream[0]["t"]
     return _summary(lat, samples, makespan)
+
+
+SWEEP_TRIANGLES = (36, 262144, 1048576, 4194304)
+
+
+def sweep(rates=(10, 50, 100, 200, 500), max_requests=10000, max_seconds=60.0, budget_gb=150, seed=7, device=0, plain=True, out=None):
+    """The serving configuration: a Poisson request stream over four resident scenes (the 36-triangle
+    box and terrain scenes of 262,144, 1,048,576 and 4,194,304 triangles), one run per rate with
+    min(max_requests, rate x max_seconds) requests, through the server and (optionally) through plain
+    renderers one request at a time. Yields one dict per rate; both forms first take a warm-up burst of
+    64 requests of another stream."""
+    import json
+    from . import workloads
+    scenes = []
+    for n in SWEEP_TRIANGLES:
+        g = native.box_scene() if n == 36 else native.terrain_scene(n, 1)
+        scenes.append((g, g.build()))
+    server = native.Server(budget_bytes=int(budget_gb) << 30, device=device)
+    ids = [server.add_scene(b.desc) for _, b in scenes]
+    plain_r = {}
+    if plain:
+        for sid, (_, b) in zip(ids, scenes):
+            r = native.Renderer(device)
+            r.upload(b.desc)
+            plain_r[sid] = r
+    pairs = [(sid, b.desc) for sid, (_, b) in zip(ids, scenes)]
+    warm = [dict(x, t=0.0) for x in workloads.request_stream(pairs, 64, 100.0, seed=seed + 1000)]
+    run_served(server, warm)
+    if plain:
+        run_plain(plain_r, warm)
+    for rate in rates:
+        n = int(min(max_requests, rate * max_seconds))
+        stream = workloads.request_stream(pairs, n, float(rate), seed=seed)
+        rec = {"rate_per_s": rate, "requests": n, "served": run_served(server, stream)}
+        if plain:
+            rec["plain"] = run_plain(plain_r, stream)
+        if out:
+            print(json.dumps(rec), file=out, flush=True)
+        yield rec
+    server.close()
+    for r in plain_r.values():
+        r.close()
+
+
+def main(argv=None):
+    import argparse
+    import sys
+    ap = argparse.ArgumentParser(description="Serving sweep: Poisson streams over four resident scenes, served vs plain.")
+    ap.add_argument("--rates", default="10,50,100,200,500")
+    ap.add_argument("--max-requests", type=int, default=10000)
+    ap.add_argument("--max-seconds", type=float, default=60.0)
+    ap.add_argument("--no-plain", action="store_true")
+    a = ap.parse_args(argv)
+    rates = [float(x) for x in a.rates.split(",")]
+    for _ in sweep(rates, a.max_requests, a.max_seconds, plain=not a.no_plain, out=sys.stdout):
+        pass
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(main())
