@@ -43,14 +43,19 @@ def dist_info():
     return world, rank, local
 
 
-def init_dist(world, local):
+def init_dist(world, local, backend="nccl"):
+    """One process per GPU (torchrun's env). NCCL carries only the barrier and the max-over-ranks
+    time; the data path has no collective. `backend="gloo"` runs the same host logic on CPU."""
     if world <= 1:
         return None
     import datetime
     import torch
     import torch.distributed as dist
-    torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    else:
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
     return dist
 
 
@@ -58,9 +63,16 @@ def reduce_max(dist, value, local):
     if dist is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    device = f"cuda:{local}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_rate(world, steps, units_per_step, max_seconds):
+    """Millions of units per second for the whole job: every rank processes `steps` x
+    `units_per_step` (weak scaling), and the job takes the slowest rank's time."""
+    return world * steps * units_per_step / max_seconds / 1e6
 
 
 def barrier(dist):
@@ -305,7 +317,7 @@ def main():
     prof = r.profile()
     total_ms = reduce_max(dist, float(sum(step_ms)), local)
     samples_per_step = WIDTH * HEIGHT * SPP
-    value = world * args.steps * samples_per_step / (total_ms / 1000.0) / 1e6
+    value = whole_job_rate(world, args.steps, samples_per_step, total_ms / 1000.0)
 
     # End to end through the C ABI: render + download into a host buffer, wall clock (no profiling).
     r.set_profiling(0)
@@ -320,7 +332,7 @@ def main():
         e2e_t.append(time.perf_counter() - t0)
     host[...] = img
     e2e_total = reduce_max(dist, float(sum(e2e_t)), local)
-    e2e_value = world * args.steps * samples_per_step / e2e_total / 1e6
+    e2e_value = whole_job_rate(world, args.steps, samples_per_step, e2e_total)
 
     # Roofline of the dominant kernel.
     kernels = {"setup": prof.setup.ms, "generate": prof.generate.ms, "trace": prof.trace.ms, "shade": prof.shade.ms,
