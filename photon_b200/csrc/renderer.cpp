@@ -676,7 +676,7 @@ void Renderer::autotune(const pt_camera& cam, const pt_render_settings& rs, int 
         }
         engine_->set_tuning(best);
     };
-    try_knob([](Tuning& t, int v) { t.path_capacity = v; }, {1 << 19, 1 << 20, 1 << 21, 1 << 22});
+    try_knob([](Tuning& t, int v) { t.path_capacity = v; }, {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24});
     try_knob([](Tuning& t, int v) { t.trace_block = v; }, {64, 128, 256});
     try_knob([](Tuning& t, int v) { t.shade_block = v; }, {64, 128, 256});
     try_knob([](Tuning& t, int v) { t.sort_by_material = v; }, {0, 1, 2, 4});

@@ -16,7 +16,7 @@ class SvgfDenoiser;
 
 // Tunable launch parameters (the autotuner's knobs).
 struct Tuning {
-    int path_capacity = 1 << 21;   // paths in flight
+    int path_capacity = 1 << 24;   // paths in flight (the pool grows to what a render needs, up to this)
     int trace_block = 128;
     int shade_block = 256;
     int sort_by_material = 4;      // shade windows of 4 x shade_block paths grouped by material class
