@@ -34,6 +34,10 @@ WORKLOAD = "262,144-triangle terrain scene (value-noise height field + 200 insta
            "64 emitters, 4 punctual lights, 1024x512 HDR sky), 1920x1080, 16 spp, max depth 12, seed 1"
 # Algorithmic bytes of the traversal kernels: one 64-byte node per visit, one 48-byte triangle per test.
 NODE_BYTES, TRI_BYTES = 64, 48
+# DRAM bytes (read + write) of all k_trace launches of one frame of this workload, from one ncu capture
+# (profiles/launches_terrain262k_1080p_16spp.md): mostly the path state streaming in and the hits out;
+# the nodes and triangles stay in L2.
+TRACE_DRAM_BYTES_PER_FRAME = 2.744e9
 
 
 def dist_info():
@@ -345,7 +349,8 @@ def main():
     achieved = (trace_bytes_per_frame * args.steps) / (prof.trace.ms / 1000.0) / 1e9 if prof.trace.ms > 0 else 0.0
     roofline = {"bound": "hbm", "kernel": "k_trace (closest-hit BVH traversal)", "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
-                "traffic": None,
+                "traffic": TRACE_DRAM_BYTES_PER_FRAME * args.steps / trace_launches,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one frame's k_trace launches",
                 "algorithmic_bytes_per_launch": trace_bytes_per_frame * args.steps / trace_launches,
                 "avg_launch_ms": prof.trace.ms / trace_launches,
                 "model": "64 B per node visit + 48 B per triangle test (closest-hit rays)",
