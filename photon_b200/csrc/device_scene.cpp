@@ -6,6 +6,7 @@
 // (lights.h:34-37) and the per-row sinf of the environment distribution (lights.h:70,94), plus the
 // luminance of each environment texel (math.h:112), so the device never needs those transcendentals.
 #include "device_scene.h"
+#include "wide_bvh.h"
 
 #include <cmath>
 #include <cstring>
@@ -84,7 +85,7 @@ size_t DeviceScene::estimate_bytes(const pt_scene_desc& d) {
 }
 
 size_t DeviceScene::device_bytes() const {
-    return nodes_.bytes() + tris_.bytes() + normals_.bytes() + tangents_.bytes() + materials_.bytes() + alias_.bytes() +
+    return nodes_.bytes() + nodes4_.bytes() + tris_.bytes() + normals_.bytes() + tangents_.bytes() + materials_.bytes() + alias_.bytes() +
            punctual_.bytes() + env_texels_.bytes() + tri_idx_.bytes() + textures_.bytes() + uvs_.bytes() + texels_.bytes() +
            srgb_lut_.bytes() + env_marginal_.bytes() + env_conditional_.bytes() + env_row_sin_.bytes() + emissive_.bytes() +
            shade_keys_.bytes() + d_view_.bytes();
@@ -96,6 +97,16 @@ void DeviceScene::upload(const pt_scene_desc& d, cudaStream_t s, bool lights_onl
     validate_scene(d, lights_only);
     if (!lights_only) {
         nodes_.upload(reinterpret_cast<const float4*>(d.nodes), size_t(d.num_nodes) * 4, s);
+        // The 4-wide BVH for any-hit rays, collapsed from the same tree (absent if it does not fit
+        // the walk's stack or leaf encoding; the shadow rays then walk the BVH2).
+        std::vector<Bvh4Node> wide;
+        int depth = 0;
+        if (build_bvh4(d.nodes, d.num_nodes, d.num_tris, wide, &depth)) {
+            nodes4_.upload(reinterpret_cast<const float4*>(wide.data()), wide.size() * 8, s);
+            PTW_CUDA(cudaStreamSynchronize(s));
+        } else {
+            nodes4_.release();
+        }
         num_vertices_ = d.num_vertices;
         if (d.normals) {
             std::vector<float4> n(size_t(d.num_vertices));
@@ -168,6 +179,7 @@ void DeviceScene::upload(const pt_scene_desc& d, cudaStream_t s, bool lights_onl
     DevScene& v = view_;
     v = DevScene{};
     v.nodes = nodes_.ptr;
+    v.nodes4 = nodes4_.ptr;
     v.tris = tris_.ptr;
     v.tri_idx = tri_idx_.ptr;
     v.normals = normals_.ptr;

@@ -91,6 +91,7 @@ public:
     static size_t estimate_bytes(const pt_scene_desc& d);
 
 private:
+    DeviceBuffer<float4> nodes4_;
     DeviceBuffer<float4> nodes_, tris_, normals_, tangents_, materials_, alias_, punctual_, env_texels_;
     DeviceBuffer<int4> tri_idx_, textures_;
     DeviceBuffer<float2> uvs_;

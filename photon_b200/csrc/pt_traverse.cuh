@@ -233,4 +233,113 @@ PT_HD bool traverse(const DevScene& s, V3 o, V3 d, float tmax, Hit& hit, int* st
     return w.tri >= 0;
 }
 
+// ---- any-hit walk over the 4-wide BVH (wide_bvh.h) -----------------------------------------------------
+// Whether some triangle accepts the ray within (0, tmax): the set of leaves a ray reaches is the
+// BVH2's (every 4-wide box is a BVH2 box, tested with the same slab arithmetic, and a box test that
+// passes also passes for the boxes containing it), and an any-hit answer does not depend on the order
+// in which they are visited. The one difference in principle: a leaf reached through an interior
+// BVH2 child whose entry distance equals tmax exactly is tested here, and Photon's walk stops at that
+// child (its `t < tmax` test); the leaf's own entry is then tmax as well.
+// One unit per step: a node visit (four slab tests; interior children pushed, then leaf children,
+// so leaves are tested first) or one triangle test. Stack entries: a node index, or a leaf as
+// 0x80000000 | count << 24 | first triangle.
+constexpr int kBvh4Stack = 96;  // = kBvh4StackSize of the builder
+
+template <bool Count, bool Packed = true>
+struct AnyWalker4 {
+    V3 o, d, inv_d;
+    RayPairs rp;
+    float tmax;
+    int node;  // the node to visit (node mode)
+    int sp;
+    int ti, te;
+    bool leaf_mode, done, hit;
+
+    PT_HD void init(V3 o_, V3 d_, float tmax_) {
+        o = o_;
+        d = d_;
+        inv_d = V3{safe_inv(d.x), safe_inv(d.y), safe_inv(d.z)};
+        rp = ray_pairs(o, inv_d);
+        tmax = tmax_;
+        node = 0;
+        sp = 0;
+        ti = te = 0;
+        leaf_mode = done = hit = false;
+    }
+    PT_HD void push(int e, int* stack, int stride, int* overflow) {
+        if (sp < kSmemStack) stack[sp * stride] = e;
+        else overflow[sp - kSmemStack] = e;
+        sp++;
+    }
+    PT_HD void pop(int* stack, int stride, int* overflow) {
+        if (sp == 0) {
+            done = true;
+            return;
+        }
+        --sp;
+        int e = sp < kSmemStack ? stack[sp * stride] : overflow[sp - kSmemStack];
+        if (e < 0) {
+            leaf_mode = true;
+            ti = e & 0xffffff;
+            te = ti + ((e >> 24) & 0x7f);
+        } else {
+            leaf_mode = false;
+            node = e;
+        }
+    }
+    PT_HD bool step(const DevScene& s, int* stack, int stride, int* overflow, TraversalCounters* cnt) {
+        if (!leaf_mode) {
+            const float4* n = s.nodes4 + 8 * node;
+            const float4 lx = __ldg(n), ly = __ldg(n + 1), lz = __ldg(n + 2), hx = __ldg(n + 3), hy = __ldg(n + 4), hz = __ldg(n + 5);
+            const int4 id = __ldg(reinterpret_cast<const int4*>(n + 6)), ct = __ldg(reinterpret_cast<const int4*>(n + 7));
+            if (Count) cnt->nodes++;
+            const float lxs[4] = {lx.x, lx.y, lx.z, lx.w}, lys[4] = {ly.x, ly.y, ly.z, ly.w}, lzs[4] = {lz.x, lz.y, lz.z, lz.w};
+            const float hxs[4] = {hx.x, hx.y, hx.z, hx.w}, hys[4] = {hy.x, hy.y, hy.z, hy.w}, hzs[4] = {hz.x, hz.y, hz.z, hz.w};
+            const int ids[4] = {id.x, id.y, id.z, id.w}, cts[4] = {ct.x, ct.y, ct.z, ct.w};
+            int leaves[4];
+            int nl = 0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (ids[k] < 0) continue;
+                const float4 bmin = make_float4(lxs[k], lys[k], lzs[k], 0.0f), bmax = make_float4(hxs[k], hys[k], hzs[k], 0.0f);
+                const float t = Packed ? box_entry2(bmin, bmax, rp, tmax) : box_entry(bmin, bmax, o, inv_d, tmax);
+                if (t == kInf) continue;
+                if (cts[k] > 0) leaves[nl++] = int(0x80000000u | (uint32_t(cts[k]) << 24) | uint32_t(ids[k]));
+                else if (t < tmax) push(ids[k], stack, stride, overflow);
+            }
+            for (int k = 0; k < nl; k++) push(leaves[k], stack, stride, overflow);
+            pop(stack, stride, overflow);
+            if (done) return false;
+        }
+        if (leaf_mode) {
+            const int i = ti;
+            const float4* g = s.tris + 3 * i;
+            float4 g0 = __ldg(g), g1 = __ldg(g + 1), g2 = __ldg(g + 2);
+            float t, tu, tv;
+            if (Count) cnt->tris++;
+            if (tri_intersect(g0, g1, g2, o, d, tmax, t, tu, tv) &&
+                !((__float_as_int(g1.w) & 1) && alpha_passes(s, i, __float_as_int(g0.w), tu, tv))) {
+                hit = true;
+                done = true;
+                return false;
+            }
+            if (++ti == te) {
+                pop(stack, stride, overflow);
+                if (done) return false;
+            }
+        }
+        return true;
+    }
+};
+
+template <bool Count, bool Packed = true>
+PT_HD bool occluded4(const DevScene& s, V3 o, V3 d, float tmax, int* stack, int stride, TraversalCounters* cnt) {
+    int overflow[kBvh4Stack - kSmemStack];
+    AnyWalker4<Count, Packed> w;
+    w.init(o, d, tmax);
+    while (w.step(s, stack, stride, overflow, cnt)) {
+    }
+    return w.hit;
+}
+
 }  // namespace ptw

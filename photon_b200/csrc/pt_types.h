@@ -17,6 +17,7 @@ namespace ptw {
 //   env       float4 per texel (rgb, luminance), row_sin per row, rotation cos/sin precomputed
 struct DevScene {
     const float4* nodes;
+    const float4* nodes4;     // the 4-wide BVH for any-hit rays (8 float4 per node), or null
     const float4* tris;
     const int4* tri_idx;
     const float4* normals;

@@ -129,6 +129,7 @@ WfParams WavefrontEngine::params(const DevScene* scenes, int single, const DevVi
     p.sort_bits = tuning_.sort_rays;
     p.sort_material = tuning_.sort_by_material;
     p.tail_paths = uint32_t(tuning_.tail_paths);
+    p.wide_shadows = tuning_.wide_shadows;
     p.keys = keys_.ptr;
     p.hist = hist_.ptr;
     p.offsets = offsets_.ptr;
@@ -613,6 +614,7 @@ void Renderer::set_tuning(const pt_tuning& t) {
     }
     if (t.packed >= 0) cur.packed = t.packed ? 1 : 0;
     if (t.tail_paths >= 0) cur.tail_paths = t.tail_paths;
+    if (t.wide_shadows >= 0) cur.wide_shadows = t.wide_shadows ? 1 : 0;
     engine_->set_tuning(cur);
 }
 
@@ -626,6 +628,7 @@ void Renderer::get_tuning(pt_tuning* t) const {
     t->sort_rays = c.sort_rays;
     t->packed = c.packed;
     t->tail_paths = c.tail_paths;
+    t->wide_shadows = c.wide_shadows;
 }
 
 // Coordinate descent over the knobs, one at a time, each candidate timed on the same probe (a view

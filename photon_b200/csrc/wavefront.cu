@@ -523,7 +523,9 @@ __global__ void __launch_bounds__(256) k_tail(const __grid_constant__ WfParams P
             if (shadow) {
                 Hit hs{kInf, -1, 0.0f, 0.0f};
                 shadow_rays++;
-                if (!traverse<true, Count, Packed>(s, sh.o, sh.d, sh.tmax, hs, stack, blockDim.x, &ts)) st.L = st.L + sh.c;
+                bool occ = (P.wide_shadows && s.nodes4) ? occluded4<Count, Packed>(s, sh.o, sh.d, sh.tmax, stack, blockDim.x, &ts)
+                                                        : traverse<true, Count, Packed>(s, sh.o, sh.d, sh.tmax, hs, stack, blockDim.x, &ts);
+                if (!occ) st.L = st.L + sh.c;
             }
             if (!cont) break;
         }
@@ -542,7 +544,7 @@ __global__ void __launch_bounds__(256) k_tail(const __grid_constant__ WfParams P
 }
 
 // ---- shadow: any hit (traverse.h:144-147) --------------------------------------------------------------
-template <bool Count, bool Packed>
+template <bool Count, bool Packed, bool Wide>
 __global__ void __launch_bounds__(256) k_shadow(const __grid_constant__ WfParams P) {
     extern __shared__ int smem_stack[];
     int* stack = smem_stack + threadIdx.x;
@@ -560,7 +562,8 @@ __global__ void __launch_bounds__(256) k_shadow(const __grid_constant__ WfParams
         uint32_t view = tag & 0x7fffffffu;
         const DevScene& s = scene_for(P, int(view));
         Hit h{kInf, -1, 0.0f, 0.0f};
-        bool occ = traverse<true, Count, Packed>(s, xyz(a), xyz(b), a.w, h, stack, blockDim.x, &tc);
+        bool occ = (Wide && s.nodes4) ? occluded4<Count, Packed>(s, xyz(a), xyz(b), a.w, stack, blockDim.x, &tc)
+                                      : traverse<true, Count, Packed>(s, xyz(a), xyz(b), a.w, h, stack, blockDim.x, &tc);
         if (!occ) {
             uint32_t target = __float_as_uint(b.w);
             if (tag & 0x80000000u) {
@@ -832,8 +835,11 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
     out->trace_block = trace_block;
     size_t smem = size_t(kSmemStack) * trace_block * sizeof(int);
     const void* smem_kernels[] = {(const void*)k_trace<false, false>, (const void*)k_trace<false, true>, (const void*)k_trace<true, false>,
-                                  (const void*)k_trace<true, true>,   (const void*)k_shadow<false, false>, (const void*)k_shadow<false, true>,
-                                  (const void*)k_shadow<true, false>, (const void*)k_shadow<true, true>};
+                                  (const void*)k_trace<true, true>,
+                                  (const void*)k_shadow<false, false, false>, (const void*)k_shadow<false, true, false>,
+                                  (const void*)k_shadow<true, false, false>, (const void*)k_shadow<true, true, false>,
+                                  (const void*)k_shadow<false, false, true>, (const void*)k_shadow<false, true, true>,
+                                  (const void*)k_shadow<true, false, true>, (const void*)k_shadow<true, true, true>};
     for (const void* k : smem_kernels) {
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
@@ -842,7 +848,7 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
     if (e != cudaSuccess) return e;
     out->trace_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
     out->shadow_block = trace_block;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shadow<false, true>, trace_block, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shadow<false, true, true>, trace_block, smem);
     if (e != cudaSuccess) return e;
     out->shadow_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
     out->shade_block = shade_block;
@@ -855,8 +861,12 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
 
 template <bool Count, bool Packed>
 static void launch_traversals(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, size_t smem, bool shadow) {
-    if (shadow) k_shadow<Count, Packed><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
-    else k_trace<Count, Packed><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
+    if (shadow) {
+        if (p.wide_shadows) k_shadow<Count, Packed, true><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
+        else k_shadow<Count, Packed, false><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
+    } else {
+        k_trace<Count, Packed><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
+    }
 }
 
 static void launch_traversal(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, size_t smem, bool shadow) {

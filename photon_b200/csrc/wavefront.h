@@ -80,6 +80,7 @@ struct WfParams {
     int packed;                // 1: f32x2 slab tests in the traversal kernels
     uint32_t tail_paths;       // > 0: once no new paths remain and at most this many are queued, finish them
                                // in one kernel (one thread per path, all bounces)
+    int wide_shadows;          // 1: shadow rays walk the 4-wide BVH where the scene has one
     int sort_material;         // 1: the shade kernel groups each block's paths by material class
     int sort_bits;             // > 0: sort continuing paths by direction octant + Morton origin cell
                                //      (this many bits per axis) before they are traced

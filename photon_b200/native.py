@@ -213,7 +213,7 @@ class Renderer:
         return p
 
     def set_tuning(self, **kw):
-        t = abi.Tuning(0, 0, 0, -1, -1, -1, -1, -1)
+        t = abi.Tuning(0, 0, 0, -1, -1, -1, -1, -1, -1)
         for k, v in kw.items():
             setattr(t, k, v)
         _check(lib.pt_set_tuning(self.h, C.byref(t)), self._err)

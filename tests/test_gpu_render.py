@@ -209,14 +209,16 @@ def test_gpu_matches_golden_fixtures(renderer, name):
     dict(trace_block=64, shade_block=64),
     dict(path_capacity=1 << 14, graph_bounces=1),
     dict(tail_paths=0),
+    dict(wide_shadows=0),
+    dict(wide_shadows=0, packed=0, tail_paths=0),
     dict(tail_paths=1 << 30),
     dict(tail_paths=1 << 12, path_capacity=1 << 14, graph_bounces=0),
 ])
 def test_tuning_variants_are_bit_identical(tuning):
     """Every autotuner knob changes how the work is scheduled, never a path's arithmetic: scalar or
     packed slab tests, material-sorted shading, ray sorting, block shapes, the path pool size, the
-    graph cadence and the one-thread-per-path tail (never, always, small) all give the same image bit
-    for bit (accumulation is in sample order)."""
+    graph cadence, the one-thread-per-path tail (never, always, small) and the shadow rays' BVH (4-wide
+    or Photon's BVH2) all give the same image bit for bit (accumulation is in sample order)."""
     desc, camf, keep = scenes.scene("terrain")
     w, h, spp = 160, 90, 4
     cam = camf(w / h)
