@@ -243,7 +243,7 @@ typedef struct pt_tuning {
     int32_t tail_paths;        /* once no new paths remain and at most this many are queued, one kernel finishes
                                   them (a thread per path, every bounce); 0 never; -1 keep */
     int32_t wide_shadows;      /* 1: shadow rays walk a 4-wide BVH collapsed from the scene's BVH2 (same
-                                  answers), 0: the BVH2; -1 keep */
+                                  answers), 0 (default): the BVH2; -1 keep */
 } pt_tuning;
 int32_t pt_set_tuning(pt_renderer* r, const pt_tuning* t);
 int32_t pt_get_tuning(const pt_renderer* r, pt_tuning* t);

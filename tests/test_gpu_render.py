@@ -209,8 +209,8 @@ def test_gpu_matches_golden_fixtures(renderer, name):
     dict(trace_block=64, shade_block=64),
     dict(path_capacity=1 << 14, graph_bounces=1),
     dict(tail_paths=0),
-    dict(wide_shadows=0),
-    dict(wide_shadows=0, packed=0, tail_paths=0),
+    dict(wide_shadows=1),
+    dict(wide_shadows=1, packed=0, tail_paths=0),
     dict(tail_paths=1 << 30),
     dict(tail_paths=1 << 12, path_capacity=1 << 14, graph_bounces=0),
 ])
