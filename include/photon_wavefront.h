@@ -343,6 +343,21 @@ int32_t pt_svgf_run_noalloc(int32_t device, int32_t width, int32_t height, const
                             const float* normal_depth, const float* position, const float* emission,
                             const pt_svgf_settings* settings, float* output, void* stream);
 
+/* ---- result encoders (host) --------------------------------------------------------------------- */
+/* PFM of a float rgb image (row-major, top row first), in the format of Photon's save_pfm
+ * (src/scene/image.cpp:88-96): "PF\n<w> <h>\n-1.0\n", then little-endian float rgb rows, bottom row
+ * first. With out == NULL only *length (the encoded size) is set; a capacity below it is
+ * PT_ERR_INVALID. */
+int32_t pt_encode_pfm(const float* rgb, int32_t width, int32_t height, uint8_t* out, size_t capacity, size_t* length);
+/* PNG (8-bit RGBA, zlib `level` 0-9) of a display buffer (pt_download_display's packing: each uint32's
+ * bytes in memory order are R, G, B, A), the image Photon's save_pfm counterpart save_png writes
+ * (image.cpp:84-86). Size query as pt_encode_pfm. */
+int32_t pt_encode_png(const uint32_t* rgba, int32_t width, int32_t height, int32_t level, uint8_t* out, size_t capacity,
+                      size_t* length);
+/* The file forms of the two encoders (photon::save_pfm / photon::save_png). */
+int32_t pt_write_pfm(const char* path, int32_t width, int32_t height, const float* rgb);
+int32_t pt_write_png(const char* path, int32_t width, int32_t height, const uint32_t* rgba);
+
 /* ---- request server (continuous batching over resident scenes) ------------------------------ */
 typedef struct pt_server pt_server;
 typedef struct pt_server_config {

@@ -76,7 +76,7 @@ def build(force=False, jobs=None, verbose=False):
             if verbose:
                 print("built", os.path.relpath(o, ROOT))
     if todo or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        cmd = [NVCC, "-shared", *GENCODE, "-o", LIB, *objs, "-cudart", "static", "-Xcompiler", "-pthread"]
+        cmd = [NVCC, "-shared", *GENCODE, "-o", LIB, *objs, "-cudart", "static", "-Xcompiler", "-pthread", "-lz"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

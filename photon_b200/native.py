@@ -71,6 +71,10 @@ def _load():
         "pt_svgf_variance": ([C.c_void_p], C.c_void_p),
         "pt_svgf_last_error": ([C.c_void_p], C.c_char_p),
         "pt_svgf_set_tma": ([C.c_void_p, C.c_int32], C.c_int32),
+        "pt_encode_pfm": ([C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, P(C.c_size_t)], C.c_int32),
+        "pt_encode_png": ([C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, P(C.c_size_t)], C.c_int32),
+        "pt_write_pfm": ([C.c_char_p, C.c_int32, C.c_int32, C.c_void_p], C.c_int32),
+        "pt_write_png": ([C.c_char_p, C.c_int32, C.c_int32, C.c_void_p], C.c_int32),
         "pt_svgf_run_noalloc": ([C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  P(abi.SvgfSettings), C.c_void_p, C.c_void_p], C.c_int32),
         "pt_server_create": ([P(abi.ServerConfig), P(C.c_void_p)], C.c_int32),
@@ -293,6 +297,28 @@ def svgf_run_noalloc(width, height, color, albedo, normal_depth, position, emiss
     device addresses (ints) of width*height float4 buffers; the call enqueues on `stream`."""
     _check(lib.pt_svgf_run_noalloc(device, width, height, color, albedo, normal_depth, position, emission, C.byref(settings),
                                    output, stream), lib.pt_global_error)
+
+
+def encode_pfm(rgb):
+    """PFM bytes of a float32 (h, w, 3) image (pt_encode_pfm)."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    h, w = rgb.shape[:2]
+    n = C.c_size_t()
+    _check(lib.pt_encode_pfm(rgb.ctypes.data, w, h, None, 0, C.byref(n)), lib.pt_global_error)
+    out = np.empty(n.value, np.uint8)
+    _check(lib.pt_encode_pfm(rgb.ctypes.data, w, h, out.ctypes.data, out.size, C.byref(n)), lib.pt_global_error)
+    return out.tobytes()
+
+
+def encode_png(rgba, level=6):
+    """PNG bytes of a uint32 (h, w) display buffer (pt_encode_png)."""
+    rgba = np.ascontiguousarray(rgba, np.uint32)
+    h, w = rgba.shape
+    n = C.c_size_t()
+    _check(lib.pt_encode_png(rgba.ctypes.data, w, h, level, None, 0, C.byref(n)), lib.pt_global_error)
+    out = np.empty(n.value, np.uint8)
+    _check(lib.pt_encode_png(rgba.ctypes.data, w, h, level, out.ctypes.data, out.size, C.byref(n)), lib.pt_global_error)
+    return out.tobytes()
 
 
 class Server:
