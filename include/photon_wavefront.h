@@ -430,7 +430,9 @@ typedef struct pt_raw_scene {
     pt_vec3 env_color; float env_intensity, env_rotation;
 } pt_raw_scene;
 typedef struct pt_built_scene pt_built_scene;
-typedef struct pt_bvh_build_options { int32_t bins, max_leaf_size; float traversal_cost; int32_t threads; } pt_bvh_build_options;
+/* BVH build options (0 fields: defaults). gpu = 1 builds on the current CUDA device: the same tree
+ * and triangle order as the host build, bit for bit (the admission cost of a large scene in serving). */
+typedef struct pt_bvh_build_options { int32_t bins, max_leaf_size; float traversal_cost; int32_t threads; int32_t gpu; } pt_bvh_build_options;
 int32_t pt_scene_build(const pt_raw_scene* raw, const pt_bvh_build_options* opt, pt_built_scene** out);
 /* The built arrays; valid until pt_scene_free. */
 const pt_scene_desc* pt_scene_desc_of(const pt_built_scene* b);

@@ -139,7 +139,7 @@ class RawScene(C.Structure):
 
 class BvhBuildOptions(C.Structure):
     _fields_ = [("bins", C.c_int32), ("max_leaf_size", C.c_int32), ("traversal_cost", C.c_float),
-                ("threads", C.c_int32)]
+                ("threads", C.c_int32), ("gpu", C.c_int32)]
 
 
 class Stats(C.Structure):

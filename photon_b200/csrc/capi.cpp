@@ -360,6 +360,7 @@ int32_t pt_scene_build(const pt_raw_scene* raw, const pt_bvh_build_options* opt,
             if (opt->max_leaf_size > 0) o.max_leaf = opt->max_leaf_size;
             if (opt->traversal_cost > 0) o.traversal_cost = opt->traversal_cost;
             o.threads = opt->threads;
+            o.gpu = opt->gpu != 0;
         }
         build_scene(*raw, o, h->b);
         *out = h.release();

@@ -21,6 +21,7 @@
 #include <thread>
 
 #include "device_scene.h"
+#include "gpu_bvh.h"
 
 namespace ptw {
 
@@ -256,6 +257,60 @@ void set_child(pt_bvh_node& n, int side, const Node* c, int out_index) {
     }
 }
 
+// The same flatten over a tree built on the device (gpu_bvh.h).
+void set_child_flat(pt_bvh_node& n, int side, const FlatBuildNode* c, int out_index) {
+    pt_vec3 lo{kBig, kBig, kBig}, hi{-kBig, -kBig, -kBig};
+    int idx = -1, cnt = 0;
+    if (c) {
+        lo = {c->lo[0], c->lo[1], c->lo[2]};
+        hi = {c->hi[0], c->hi[1], c->hi[2]};
+        const bool leaf = c->kid[0] < 0;
+        idx = leaf ? c->first : out_index;
+        cnt = leaf ? c->count : 0;
+    }
+    if (side == 0) {
+        n.lmin = lo;
+        n.lmax = hi;
+        n.left = idx;
+        n.lcount = cnt;
+    } else {
+        n.rmin = lo;
+        n.rmax = hi;
+        n.right = idx;
+        n.rcount = cnt;
+    }
+}
+
+float box_area(const float lo[3], const float hi[3]) {
+    Box b;
+    for (int k = 0; k < 3; k++) {
+        b.lo[k] = lo[k];
+        b.hi[k] = hi[k];
+    }
+    return b.area();
+}
+
+void flatten_flat(const std::vector<FlatBuildNode>& tree, int n, int out_index, int depth, std::vector<pt_bvh_node>& out, BvhInfo& info,
+                  float root_area, float trav) {
+    info.nodes++;
+    info.max_depth = std::max(info.max_depth, depth);
+    for (int side = 0; side < 2; side++) {
+        const FlatBuildNode* c = &tree[size_t(tree[size_t(n)].kid[side])];
+        const bool leaf = c->kid[0] < 0;
+        int child_out = -1;
+        if (!leaf) {
+            child_out = int(out.size());
+            out.push_back(pt_bvh_node{});
+            info.sah_cost += trav * box_area(c->lo, c->hi) / root_area;
+        } else {
+            info.leaves++;
+            info.sah_cost += float(c->count) * box_area(c->lo, c->hi) / root_area;
+        }
+        set_child_flat(out[size_t(out_index)], side, c, child_out);
+        if (!leaf) flatten_flat(tree, tree[size_t(n)].kid[side], child_out, depth + 1, out, info, root_area, trav);
+    }
+}
+
 // Depth-first flatten: each output node holds the two children of an interior build node.
 void flatten(const Node* n, int out_index, int depth, std::vector<pt_bvh_node>& out, BvhInfo& info, float root_area, float trav) {
     info.nodes++;
@@ -432,6 +487,34 @@ void build_scene(const pt_raw_scene& raw, const BvhOptions& opt, BuiltScene& out
         set_child(r, 0, nullptr, -1);
         set_child(r, 1, nullptr, -1);
         out.nodes.push_back(r);
+    } else if (opt.gpu) {
+        std::vector<float> flat_boxes(6 * size_t(n));
+        for (int t = 0; t < n; t++)
+            for (int k = 0; k < 3; k++) {
+                flat_boxes[6 * size_t(t) + size_t(k)] = boxes[size_t(t)].lo[k];
+                flat_boxes[6 * size_t(t) + 3 + size_t(k)] = boxes[size_t(t)].hi[k];
+            }
+        int device = 0;
+        PTW_CUDA(cudaGetDevice(&device));
+        std::vector<FlatBuildNode> tree;
+        gpu_build_bvh(device, flat_boxes, cent, n, std::max(2, std::min(opt.bins, 64)), opt.max_leaf, opt.traversal_cost, order, tree);
+        const FlatBuildNode& r = tree[0];
+        for (int k = 0; k < 3; k++) {
+            root_box.lo[k] = r.lo[k];
+            root_box.hi[k] = r.hi[k];
+        }
+        float root_area = std::max(root_box.area(), 1e-20f);
+        out.nodes.push_back(pt_bvh_node{});
+        if (r.kid[0] < 0) {
+            set_child_flat(out.nodes[0], 0, &r, -1);
+            set_child_flat(out.nodes[0], 1, nullptr, -1);
+            out.bvh.nodes = 1;
+            out.bvh.leaves = 1;
+            out.bvh.sah_cost = float(r.count);
+        } else {
+            out.bvh.sah_cost = opt.traversal_cost;
+            flatten_flat(tree, 0, 0, 0, out.nodes, out.bvh, root_area, opt.traversal_cost);
+        }
     } else {
         TaskBvhBuilder builder(boxes, cent, opt, order);
         std::unique_ptr<Node> root = builder.run(n);

@@ -15,6 +15,7 @@ struct BvhOptions {
     int max_leaf = 8;          // leaves never hold more triangles
     float traversal_cost = 1.0f;
     int threads = 0;           // 0: hardware concurrency
+    bool gpu = false;          // build on the current CUDA device (the same tree)
 };
 
 struct BvhInfo {

@@ -544,8 +544,10 @@ __global__ void __launch_bounds__(256) k_tail(const __grid_constant__ WfParams P
 }
 
 // ---- shadow: any hit (traverse.h:144-147) --------------------------------------------------------------
+// Capped at 51 registers (five 256-thread blocks per SM): the any-hit walk gains more from the extra
+// resident warps than it loses to the tighter allocation (measured; the closest-hit walk does not).
 template <bool Count, bool Packed, bool Wide>
-__global__ void __launch_bounds__(256) k_shadow(const __grid_constant__ WfParams P) {
+__global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfParams P) {
     extern __shared__ int smem_stack[];
     int* stack = smem_stack + threadIdx.x;
     Counters* c = P.ctr;

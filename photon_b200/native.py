@@ -382,9 +382,9 @@ class Server:
 class BuiltScene:
     """Raw meshes built into a pt_scene_desc by the library's own builder."""
 
-    def __init__(self, raw, bins=0, max_leaf=0, traversal_cost=0.0, threads=0, keepalive=None):
+    def __init__(self, raw, bins=0, max_leaf=0, traversal_cost=0.0, threads=0, gpu=False, keepalive=None):
         p = C.c_void_p()
-        o = abi.BvhBuildOptions(bins, max_leaf, traversal_cost, threads)
+        o = abi.BvhBuildOptions(bins, max_leaf, traversal_cost, threads, 1 if gpu else 0)
         _check(lib.pt_scene_build(C.byref(raw), C.byref(o), C.byref(p)), lib.pt_global_error)
         self.h = p
         self._keep = keepalive
