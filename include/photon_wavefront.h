@@ -363,7 +363,7 @@ typedef struct pt_server pt_server;
 typedef struct pt_server_config {
     int32_t device;
     uint64_t budget_bytes;     /* device memory for scenes + requests + path pool */
-    int32_t path_capacity;     /* shared path pool (0: 2,097,152 paths) */
+    int32_t path_capacity;     /* shared path pool (0: 8,388,608 paths) */
     int32_t max_active;        /* requests on the device at once (0: unbounded, budget only) */
     double device_wait_seconds;/* bound of every device-side wait (0: 2 s) */
 } pt_server_config;

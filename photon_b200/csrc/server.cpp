@@ -33,9 +33,10 @@ Server::Server(const pt_server_config& cfg) : cfg_(cfg), device_(cfg.device) {
     PTW_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     engine_ = std::make_unique<WavefrontEngine>(device_, stream_);
     // The server keeps a smaller pool than a plain render: the work handed over ahead of generation
-    // is a few pools, and a new request waits behind it.
+    // is a few pools, and a new request waits behind it (8M paths measured best for p99 latency and
+    // throughput on the mixed stream).
     Tuning t;
-    t.path_capacity = cfg.path_capacity > 0 ? cfg.path_capacity : (1 << 21);
+    t.path_capacity = cfg.path_capacity > 0 ? cfg.path_capacity : (1 << 23);
     engine_->set_tuning(t);
     engine_->reserve_paths(uint64_t(t.path_capacity));
     pool_bytes_ = engine_->device_bytes();
