@@ -343,6 +343,20 @@ int32_t pt_svgf_run_noalloc(int32_t device, int32_t width, int32_t height, const
                             const float* normal_depth, const float* position, const float* emission,
                             const pt_svgf_settings* settings, float* output, void* stream);
 
+/* Light tables rebuilt on the device (no counterpart call in Photon, whose update_lights takes a scene
+ * rebuilt on the host: gpu_renderer.cu:299-334 after scene.cpp:113-210). New materials (same count,
+ * same per-triangle assignment), punctual lights and environment for the uploaded scene; the
+ * emissive-triangle list, its alias table, the light-group probabilities and the environment's
+ * sampling distribution are computed on the device, equal to what pt_scene_build computes for the
+ * same inputs. env_texels NULL: a constant environment of env_color. */
+typedef struct pt_light_update {
+    const pt_material* materials; int32_t num_materials;
+    const pt_punctual_light* punctual; int32_t num_punctual;
+    const pt_vec3* env_texels; int32_t env_width, env_height;
+    pt_vec3 env_color; float env_intensity, env_rotation;
+} pt_light_update;
+int32_t pt_rebuild_lights(pt_renderer* r, const pt_light_update* update);
+
 /* ---- result encoders (host) --------------------------------------------------------------------- */
 /* PFM of a float rgb image (row-major, top row first), in the format of Photon's save_pfm
  * (src/scene/image.cpp:88-96): "PF\n<w> <h>\n-1.0\n", then little-endian float rgb rows, bottom row

@@ -142,6 +142,13 @@ class BvhBuildOptions(C.Structure):
                 ("threads", C.c_int32), ("gpu", C.c_int32)]
 
 
+class LightUpdate(C.Structure):
+    _fields_ = [("materials", C.POINTER(Material)), ("num_materials", C.c_int32),
+                ("punctual", C.POINTER(PunctualLight)), ("num_punctual", C.c_int32),
+                ("env_texels", C.POINTER(Vec3)), ("env_width", C.c_int32), ("env_height", C.c_int32),
+                ("env_color", Vec3), ("env_intensity", C.c_float), ("env_rotation", C.c_float)]
+
+
 class Stats(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("samples", C.c_int32), ("last_frame_ms", C.c_float),
                 ("paths", C.c_uint64), ("rays", C.c_uint64), ("shadow_rays", C.c_uint64),

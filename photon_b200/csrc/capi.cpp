@@ -142,6 +142,11 @@ int32_t pt_update_lights(pt_renderer* r, const pt_scene_desc* scene) {
     PT_RENDERER_CALL(r, r->r->upload(*scene, true));
 }
 
+int32_t pt_rebuild_lights(pt_renderer* r, const pt_light_update* update) {
+    if (!update) return PT_ERR_INVALID;
+    PT_RENDERER_CALL(r, r->r->rebuild_lights(*update));
+}
+
 int32_t pt_resize(pt_renderer* r, int32_t width, int32_t height) { PT_RENDERER_CALL(r, r->r->resize(width, height)); }
 
 int32_t pt_reset(pt_renderer* r) { PT_RENDERER_CALL(r, r->r->reset()); }

@@ -91,6 +91,24 @@ size_t DeviceScene::device_bytes() const {
            shade_keys_.bytes() + d_view_.bytes();
 }
 
+// Shading classes: materials of one class take the same branches through the BSDF, texture and
+// emission code, so the shade kernel groups a block's paths by class.
+void DeviceScene::upload_shade_keys(const pt_material* materials, int32_t n, cudaStream_t s) {
+    std::vector<uint8_t> keys(static_cast<size_t>(n));
+    for (size_t m = 0; m < keys.size(); m++) {
+        const pt_material& mm = materials[m];
+        int k = 1;
+        if (mm.metallic > 0.0f) k += 1;
+        if (mm.transmission > 0.0f) k += 2;
+        if (mm.base_color_tex >= 0 || mm.metallic_roughness_tex >= 0) k += 4;
+        if (mm.normal_tex >= 0) k += 8;
+        if (mm.emission.x > 0.0f || mm.emission.y > 0.0f || mm.emission.z > 0.0f || mm.emissive_tex >= 0) k += 16;
+        keys[m] = uint8_t(k);
+    }
+    shade_keys_.upload(keys.data(), keys.size(), s);
+    PTW_CUDA(cudaStreamSynchronize(s));
+}
+
 void DeviceScene::upload(const pt_scene_desc& d, cudaStream_t s, bool lights_only) {
     if (lights_only && !ready_) lights_only = false;
     if (lights_only && d.num_tris != view_.num_tris) throw Error{PT_ERR_INVALID, "update_lights: the triangle count changed"};
@@ -136,21 +154,8 @@ void DeviceScene::upload(const pt_scene_desc& d, cudaStream_t s, bool lights_onl
     // and the environment.
     tris_.upload(reinterpret_cast<const float4*>(d.tris), size_t(d.num_tris) * 3, s);
     materials_.upload(reinterpret_cast<const float4*>(d.materials), size_t(d.num_materials) * 5, s);
-    // Shading classes: materials of one class take the same branches through the BSDF, texture and
-    // emission code, so the shade kernel groups a block's paths by class.
-    std::vector<uint8_t> keys(size_t(d.num_materials));
-    for (size_t m = 0; m < keys.size(); m++) {
-        const pt_material& mm = d.materials[m];
-        int k = 1;
-        if (mm.metallic > 0.0f) k += 1;
-        if (mm.transmission > 0.0f) k += 2;
-        if (mm.base_color_tex >= 0 || mm.metallic_roughness_tex >= 0) k += 4;
-        if (mm.normal_tex >= 0) k += 8;
-        if (mm.emission.x > 0.0f || mm.emission.y > 0.0f || mm.emission.z > 0.0f || mm.emissive_tex >= 0) k += 16;
-        keys[m] = uint8_t(k);
-    }
-    shade_keys_.upload(keys.data(), keys.size(), s);
-    PTW_CUDA(cudaStreamSynchronize(s));
+    num_materials_ = d.num_materials;
+    upload_shade_keys(d.materials, d.num_materials, s);
     std::vector<int4> idx(size_t(d.num_tris));
     for (size_t t = 0; t < idx.size(); t++)
         idx[t] = make_int4(d.indices[3 * t], d.indices[3 * t + 1], d.indices[3 * t + 2], d.tri_emissive ? d.tri_emissive[t] : -1);
@@ -237,6 +242,12 @@ void DeviceScene::upload(const pt_scene_desc& d, cudaStream_t s, bool lights_onl
     }
     d_view_.upload(&v, 1, s);
     PTW_CUDA(cudaStreamSynchronize(s));
+    bounds_[0] = d.bounds_min.x;
+    bounds_[1] = d.bounds_min.y;
+    bounds_[2] = d.bounds_min.z;
+    bounds_[3] = d.bounds_max.x;
+    bounds_[4] = d.bounds_max.y;
+    bounds_[5] = d.bounds_max.z;
     float dx = d.bounds_max.x - d.bounds_min.x, dy = d.bounds_max.y - d.bounds_min.y, dz = d.bounds_max.z - d.bounds_min.z;
     extent_ = std::fmax(std::sqrt(dx * dx + dy * dy + dz * dz), 1e-3f);
     if (!std::isfinite(extent_)) extent_ = 1.0f;

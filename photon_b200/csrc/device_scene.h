@@ -89,6 +89,9 @@ public:
     float extent() const { return extent_; }
     // Bytes a scene will occupy on the device (for admission before upload).
     static size_t estimate_bytes(const pt_scene_desc& d);
+    // pt_rebuild_lights: new materials, punctual lights and environment; the light tables are built
+    // on the device (light_build.cu).
+    void rebuild_lights(const pt_light_update& u, cudaStream_t stream);
 
 private:
     DeviceBuffer<float4> nodes4_;
@@ -104,6 +107,9 @@ private:
     bool ready_ = false;
     float extent_ = 1.0f;
     int32_t num_vertices_ = 0;
+    int32_t num_materials_ = 0;
+    void upload_shade_keys(const pt_material* materials, int32_t n, cudaStream_t s);
+    float bounds_[6] = {0, 0, 0, 0, 0, 0};  // the scene box (lo xyz, hi xyz), for the light-group weights
 };
 
 // Checks a scene description for internal consistency; throws Error(PT_ERR_INVALID).

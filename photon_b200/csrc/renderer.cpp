@@ -286,6 +286,12 @@ void Renderer::upload(const pt_scene_desc& d, bool lights_only) {
     }
 }
 
+void Renderer::rebuild_lights(const pt_light_update& u) {
+    PTW_CUDA(cudaSetDevice(device_));
+    scene_.rebuild_lights(u, stream_);
+    if (width_ > 0) reset();
+}
+
 void Renderer::resize(int w, int h) {
     if (w < 0 || h < 0) throw Error{PT_ERR_INVALID, "negative image size"};
     if (w == width_ && h == height_ && accum_.count) return;

@@ -110,6 +110,7 @@ public:
     ~Renderer();
 
     void upload(const pt_scene_desc& d, bool lights_only);
+    void rebuild_lights(const pt_light_update& u);
     void resize(int w, int h);
     void reset();
     void render(const pt_camera& cam, const pt_render_settings& rs, int spp);

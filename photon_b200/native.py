@@ -71,6 +71,7 @@ def _load():
         "pt_svgf_variance": ([C.c_void_p], C.c_void_p),
         "pt_svgf_last_error": ([C.c_void_p], C.c_char_p),
         "pt_svgf_set_tma": ([C.c_void_p, C.c_int32], C.c_int32),
+        "pt_rebuild_lights": ([C.c_void_p, P(abi.LightUpdate)], C.c_int32),
         "pt_encode_pfm": ([C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, P(C.c_size_t)], C.c_int32),
         "pt_encode_png": ([C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, P(C.c_size_t)], C.c_int32),
         "pt_write_pfm": ([C.c_char_p, C.c_int32, C.c_int32, C.c_void_p], C.c_int32),
@@ -157,6 +158,10 @@ class Renderer:
 
     def render(self, cam, rs, spp):
         _check(lib.pt_render(self.h, C.byref(cam), C.byref(rs), spp), self._err)
+
+    def rebuild_lights(self, update):
+        """pt_rebuild_lights with an abi.LightUpdate."""
+        _check(lib.pt_rebuild_lights(self.h, C.byref(update)), self._err)
 
     def render_denoised(self, cam, prev, rs, sv):
         _check(lib.pt_render_denoised(self.h, C.byref(cam), C.byref(prev), C.byref(rs), C.byref(sv)), self._err)
