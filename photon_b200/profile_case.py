@@ -2,6 +2,7 @@
 resolution, launched without CUDA graphs so every kernel is an ordinary launch.
 
     python -m photon_b200.profile_case [--width 960] [--height 540] [--spp 4] [--triangles 262144]
+    python -m photon_b200.profile_case --denoise 3 --width 1600 --height 900   # real-time SVGF frames
 
 At 960x540x4 the device holds ~0.6 GB (scene 21 MB, path pool, radiance buffer), well inside an
 ncu capture's budget, and the path state (> 126 MB) still exceeds L2.
@@ -19,6 +20,7 @@ def main(argv=None):
     ap.add_argument("--spp", type=int, default=4)
     ap.add_argument("--triangles", type=int, default=262144)
     ap.add_argument("--depth", type=int, default=12)
+    ap.add_argument("--denoise", type=int, default=0, help="render this many real-time SVGF frames instead")
     a = ap.parse_args(argv)
     g = native.terrain_scene(a.triangles, 1)
     b = g.build()
@@ -28,6 +30,15 @@ def main(argv=None):
     r.upload(b.desc)
     r.resize(a.width, a.height)
     r.set_tuning(graph_bounces=0)
+    if a.denoise:
+        from . import workloads
+        cams = workloads.orbit_cameras(b.desc, a.denoise, a.width / a.height)
+        for f in range(a.denoise):
+            r.render_denoised(cams[f], cams[max(f - 1, 0)], rs, abi.svgf_settings())
+        st = r.stats()
+        print(f"rendered {a.denoise} denoised {a.width}x{a.height} frames, last {st.last_frame_ms:.2f} ms")
+        r.close()
+        return 0
     r.render(cam, rs, a.spp)
     st = r.stats()
     print(f"rendered {a.width}x{a.height}x{a.spp}: {st.bounce_iterations} iterations, {st.rays} rays, {st.last_frame_ms:.2f} ms")
