@@ -691,7 +691,7 @@ void Renderer::autotune(const pt_camera& cam, const pt_render_settings& rs, int 
     try_knob([](Tuning& t, int v) { t.sort_by_material = v; }, {0, 1, 2, 4});
     try_knob([](Tuning& t, int v) { t.graph_bounces = v; }, {2, 4, 8});
     try_knob([](Tuning& t, int v) { t.sort_rays = v; }, {0, 3});
-    try_knob([](Tuning& t, int v) { t.tail_paths = v; }, {0, 1 << 16, 1 << 18, 1 << 20});
+    try_knob([](Tuning& t, int v) { t.tail_paths = v; }, {0, 1 << 16, 1 << 17, 1 << 18, 1 << 20});
     try_knob([](Tuning& t, int v) { t.wide_shadows = v; }, {0, 1});
     engine_->set_tuning(best);
     batch_views_ = saved_views;

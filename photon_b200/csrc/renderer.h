@@ -24,7 +24,7 @@ struct Tuning {
     int sort_rays = 0;             // origin bits per axis of the ray-sort key (0: no sorting)
     int packed = 1;                // f32x2 slab tests
     int wide_shadows = 0;          // 1: shadow rays walk the 4-wide BVH (measured slower on the 262K scene)
-    int tail_paths = 1 << 16;      // finish the last queued paths one thread each below this many (0: never)
+    int tail_paths = 1 << 17;      // finish the last queued paths one thread each below this many (0: never)
 };
 
 // Runs wavefront passes over a table of views on one device stream. Owns the path pool, the
