@@ -357,6 +357,11 @@ def main():
                 "node_visits_per_ray": counts.closest_node_visits / max(1, counts.closest_rays),
                 "tri_tests_per_ray": counts.closest_tri_tests / max(1, counts.closest_rays),
                 "shadow_bytes_per_frame": shadow_bytes_per_frame}
+    # The scene stays in L2, so the same bytes are also read against a live L2 read probe.
+    l2_peak = native.l2_read_bandwidth(local)
+    roofline["l2"] = {"peak": l2_peak, "unit": "GB/s", "frac": achieved / l2_peak if l2_peak > 0 else None,
+                      "peak_source": "live pt_measure_l2_bandwidth: 32 MiB L2-resident buffer read 64 times per "
+                                     "launch (ld.global.cg), best of 5"}
     rays_per_sample = (counts.closest_rays + counts.shadow_rays) / samples_per_step
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

@@ -241,7 +241,9 @@ typedef struct pt_tuning {
                                   with this many bits per axis before tracing them; -1 keep */
     int32_t packed;            /* 1: f32x2 (packed FP32) slab tests in traversal, 0: scalar; -1 keep */
     int32_t tail_paths;        /* once no new paths remain and at most this many are queued, one kernel finishes
-                                  them (a thread per path, every bounce); 0 never; -1 keep */
+                                  them (a thread per path, every bounce); 0 never; -1 keep; -2 (default)
+                                  131,072 for a render that starts while no other render of this process
+                                  runs on the device, 65,536 otherwise and in the server */
     int32_t wide_shadows;      /* 1: shadow rays walk a 4-wide BVH collapsed from the scene's BVH2 (same
                                   answers), 0 (default): the BVH2; -1 keep */
 } pt_tuning;
@@ -259,6 +261,11 @@ int32_t pt_autotune(pt_renderer* r, const pt_camera* camera, const pt_render_set
 /* The CUDA stream (a cudaStream_t) on which every device operation of this renderer is ordered, so
  * that callers can time it with their own events. */
 void* pt_renderer_stream(pt_renderer* r);
+
+/* Read bandwidth (GB/s) of an L2-resident buffer of `bytes` (1 MiB to 64 MiB) read `reps` times per
+ * launch with loads that bypass L1; the best of five launches. The denominator for kernels whose
+ * data stays in L2 (the BVH walk). No counterpart in Photon (a measurement helper). */
+int32_t pt_measure_l2_bandwidth(int32_t device, size_t bytes, int32_t reps, double* gbs);
 
 enum { PT_PROFILE_KERNEL_TIMES = 1, PT_PROFILE_TRAVERSAL_COUNTS = 2 };
 typedef struct pt_kernel_time { uint64_t launches; double ms; } pt_kernel_time;

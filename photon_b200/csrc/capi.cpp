@@ -6,6 +6,7 @@
 #include <new>
 #include <string>
 
+#include "peaks.h"
 #include "photon_wavefront.h"
 #include "renderer.h"
 #include "scene_build.h"
@@ -190,6 +191,15 @@ int32_t pt_get_stats(const pt_renderer* r, pt_stats* out) {
 }
 
 void* pt_renderer_stream(pt_renderer* r) { return r && r->r ? reinterpret_cast<void*>(r->r->stream()) : nullptr; }
+
+int32_t pt_measure_l2_bandwidth(int32_t device, size_t bytes, int32_t reps, double* gbs) {
+    if (!gbs) return PT_ERR_INVALID;
+    *gbs = 0.0;
+    return guarded(nullptr, [&] {
+        require_device(device);
+        *gbs = measure_l2_read_gbs(device, bytes, reps);
+    });
+}
 
 int32_t pt_set_profiling(pt_renderer* r, int32_t flags) { PT_RENDERER_CALL(r, r->r->set_profiling(flags)); }
 

@@ -3,6 +3,7 @@
 #include "renderer.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstddef>
 #include <cstring>
@@ -12,6 +13,30 @@
 namespace ptw {
 
 // ---- WavefrontEngine ------------------------------------------------------------------------------------
+
+namespace {
+
+// Renders of this process in progress per device (WavefrontEngine::run), for the kTailAuto choice.
+constexpr int kMaxDevices = 64;
+std::atomic<int> g_renders[kMaxDevices];
+
+struct RenderCount {
+    int device;
+    int others;  // other renders in progress on the device when this one started
+    explicit RenderCount(int d) : device(d >= 0 && d < kMaxDevices ? d : -1), others(0) {
+        if (device >= 0) others = g_renders[device].fetch_add(1);
+    }
+    ~RenderCount() {
+        if (device >= 0) g_renders[device].fetch_sub(1);
+    }
+};
+
+uint32_t tail_limit(int tail_paths, bool alone) {
+    if (tail_paths == kTailAuto) return uint32_t(alone ? kTailAlone : kTailShared);
+    return tail_paths > 0 ? uint32_t(tail_paths) : 0u;
+}
+
+}  // namespace
 
 WavefrontEngine::WavefrontEngine(int device, cudaStream_t stream) : device_(device), stream_(stream) {
     PTW_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_ctr_), sizeof(Counters)));
@@ -128,7 +153,7 @@ WfParams WavefrontEngine::params(const DevScene* scenes, int single, const DevVi
     p.packed = tuning_.packed ? 1 : 0;
     p.sort_bits = tuning_.sort_rays;
     p.sort_material = tuning_.sort_by_material;
-    p.tail_paths = uint32_t(tuning_.tail_paths);
+    p.tail_paths = tuning_.tail_paths == kTailAuto ? 1u : uint32_t(std::max(0, tuning_.tail_paths));
     p.wide_shadows = tuning_.wide_shadows;
     p.keys = keys_.ptr;
     p.hist = hist_.ptr;
@@ -174,9 +199,11 @@ void WavefrontEngine::run(const DevScene* scenes, int single_scene, const DevVie
     if (stale != cudaSuccess) throw Error{PT_ERR_CUDA, std::string("an earlier CUDA call failed: ") + cudaGetErrorString(stale)};
     reserve_paths(total_work);
     ensure_shape();
+    RenderCount busy(device_);
     std::memset(h_ctr_, 0, sizeof(Counters));
     h_ctr_->parity = 1;
     h_ctr_->work_total = total_work;
+    h_ctr_->tail_limit = tail_limit(tuning_.tail_paths, busy.others == 0);
     PTW_CUDA(cudaMemcpyAsync(ctr_.ptr, h_ctr_, sizeof(Counters), cudaMemcpyHostToDevice, stream_));
     WfParams p = params(scenes, single_scene, views, n_views, count_work || (profile_flags_ & PT_PROFILE_TRAVERSAL_COUNTS));
     bool use_graph = tuning_.graph_bounces > 0;
@@ -207,6 +234,7 @@ void WavefrontEngine::begin(const DevScene* scenes, const DevView* views, int n_
     ensure_shape();
     std::memset(h_ctr_, 0, sizeof(Counters));
     h_ctr_->parity = 1;
+    h_ctr_->tail_limit = tail_limit(tuning_.tail_paths, false);  // a server shares the GPU between requests
     PTW_CUDA(cudaMemcpyAsync(ctr_.ptr, h_ctr_, sizeof(Counters), cudaMemcpyHostToDevice, stream_));
     cont_params_ = params(scenes, -1, views, n_views, false);
 }
@@ -619,7 +647,7 @@ void Renderer::set_tuning(const pt_tuning& t) {
         cur.sort_rays = t.sort_rays;
     }
     if (t.packed >= 0) cur.packed = t.packed ? 1 : 0;
-    if (t.tail_paths >= 0) cur.tail_paths = t.tail_paths;
+    if (t.tail_paths >= 0 || t.tail_paths == kTailAuto) cur.tail_paths = t.tail_paths;
     if (t.wide_shadows >= 0) cur.wide_shadows = t.wide_shadows ? 1 : 0;
     engine_->set_tuning(cur);
 }

@@ -14,6 +14,16 @@ namespace ptw {
 
 class SvgfDenoiser;
 
+// tail_paths value that picks the threshold per render: kTailAlone while no other render of this
+// process runs on the device, kTailShared otherwise. A render alone is bound by its longest paths,
+// which the tail finishes without an iteration barrier per bounce; renders that share the GPU are
+// bound by throughput, where the wavefront's sorted iterations use the SMs better than the tail's
+// one path per thread (1600x900 real-time frames: one session 3.6 -> 3.1 ms with the larger
+// threshold, eight concurrent sessions 12.6 -> 15.5 ms).
+constexpr int kTailAuto = -2;
+constexpr int kTailAlone = 1 << 17;
+constexpr int kTailShared = 1 << 16;
+
 // Tunable launch parameters (the autotuner's knobs).
 struct Tuning {
     int path_capacity = 1 << 24;   // paths in flight (the pool grows to what a render needs, up to this)
@@ -24,7 +34,7 @@ struct Tuning {
     int sort_rays = 0;             // origin bits per axis of the ray-sort key (0: no sorting)
     int packed = 1;                // f32x2 slab tests
     int wide_shadows = 0;          // 1: shadow rays walk the 4-wide BVH (measured slower on the 262K scene)
-    int tail_paths = 1 << 17;      // finish the last queued paths one thread each below this many (0: never)
+    int tail_paths = kTailAuto;    // finish the last queued paths one thread each below this many (0: never)
 };
 
 // Runs wavefront passes over a table of views on one device stream. Owns the path pool, the

@@ -114,7 +114,7 @@ __device__ __forceinline__ int find_view(const DevView* views, int n, unsigned l
 __global__ void k_setup(const __grid_constant__ WfParams P) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     Counters* c = P.ctr;
-    const uint32_t capacity = P.pb.capacity, tail_paths = P.tail_paths;
+    const uint32_t capacity = P.pb.capacity, tail_paths = P.tail_paths > 0 ? c->tail_limit : 0u;
     uint32_t p = c->parity ^ 1u;
     c->parity = p;
     uint32_t cnt = c->count[p];

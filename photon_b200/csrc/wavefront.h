@@ -48,6 +48,7 @@ struct Counters {
     uint32_t fetch[6];               // work-claim counters: generate, trace, shade, shadow, sort scatter, tail
     uint32_t overflow;
     uint32_t tail;                   // 1: this iteration finishes every queued path in k_tail
+    uint32_t tail_limit;             // queued paths at or below which k_tail takes over (host-set per render)
     uint32_t gen_view;               // first view whose work is not all generated (views are in work order)
     uint32_t iterations;
     unsigned long long work_base, work_next, work_total;
@@ -78,8 +79,8 @@ struct WfParams {
     Counters* ctr;
     int count_work;            // 1: count node visits / triangle tests (stats runs)
     int packed;                // 1: f32x2 slab tests in the traversal kernels
-    uint32_t tail_paths;       // > 0: once no new paths remain and at most this many are queued, finish them
-                               // in one kernel (one thread per path, all bounces)
+    uint32_t tail_paths;       // > 0: once no new paths remain and at most Counters::tail_limit are queued,
+                               // finish them in one kernel (one thread per path, all bounces)
     int wide_shadows;          // 1: shadow rays walk the 4-wide BVH where the scene has one
     int sort_material;         // 1: the shade kernel groups each block's paths by material class
     int sort_bits;             // > 0: sort continuing paths by direction octant + Morton origin cell

@@ -52,6 +52,7 @@ def _load():
         "pt_display_buffer": ([C.c_void_p], C.c_void_p),
         "pt_get_stats": ([C.c_void_p, P(abi.Stats)], C.c_int32),
         "pt_renderer_stream": ([C.c_void_p], C.c_void_p),
+        "pt_measure_l2_bandwidth": ([C.c_int32, C.c_size_t, C.c_int32, P(C.c_double)], C.c_int32),
         "pt_set_profiling": ([C.c_void_p, C.c_int32], C.c_int32),
         "pt_get_profile": ([C.c_void_p, P(abi.Profile)], C.c_int32),
         "pt_set_tuning": ([C.c_void_p, P(abi.Tuning)], C.c_int32),
@@ -121,6 +122,13 @@ def device_info():
     if not lib.pt_device_info(name, 256, C.byref(major), C.byref(minor), C.byref(mem), C.byref(mp)):
         return None
     return dict(name=name.value.decode(), major=major.value, minor=minor.value, memory=mem.value, multiprocessors=mp.value)
+
+
+def l2_read_bandwidth(device=0, nbytes=32 << 20, reps=64):
+    """GB/s of an L2-resident read (pt_measure_l2_bandwidth)."""
+    g = C.c_double()
+    _check(lib.pt_measure_l2_bandwidth(device, nbytes, reps, C.byref(g)), lambda: lib.pt_global_error().decode())
+    return g.value
 
 
 class Renderer:

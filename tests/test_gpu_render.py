@@ -234,3 +234,37 @@ def test_tuning_variants_are_bit_identical(tuning):
         imgs.append(r.download_image())
         r.close()
     assert np.array_equal(imgs[0], imgs[1])
+
+
+def test_adaptive_tail_is_bit_identical_alone_and_concurrent():
+    """The default tail threshold (-2) is chosen per render from how many renders of the process run
+    on the device; it moves work between kernels only, so renders alone and renders that overlap
+    on other threads give the image of a render with the tail switched off, bit for bit."""
+    import threading
+    desc, camf, keep = scenes.scene("terrain")
+    w, h, spp = 320, 180, 2
+    cam = camf(w / h)
+    rs = _settings("terrain", w, h, seed=5)
+
+    def render(tuning=None):
+        r = native.Renderer()
+        r.upload(desc)
+        r.resize(w, h)
+        if tuning:
+            r.set_tuning(**tuning)
+        assert r.tuning()["tail_paths"] == (tuning or {}).get("tail_paths", -2)
+        r.render(cam, rs, spp)
+        img = r.download_image()
+        r.close()
+        return img
+
+    ref = render(dict(tail_paths=0))
+    assert np.array_equal(render(), ref)
+    out = [None] * 4
+    threads = [threading.Thread(target=lambda k=k: out.__setitem__(k, render())) for k in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for img in out:
+        assert img is not None and np.array_equal(img, ref)
