@@ -334,8 +334,8 @@ const char* pt_svgf_last_error(const pt_svgf* s);
 
 /* An allocation-free SVGF denoise of one frame, for callers that cannot call cudaMalloc: an engine
  * whose frame loop must not allocate (allocation synchronises the device and stalls the frame), a
- * caller whose device memory is owned by its own caching allocator, code recorded into CUDA graphs
- * or run where allocation is not allowed. No counterpart in Photon (its Svgf allocates its buffers in
+ * caller whose device memory is owned by its own caching allocator, or code that runs where the
+ * CUDA allocator may not be called. No counterpart in Photon (its Svgf allocates its buffers in
  * Svgf::resize, svgf.cu:225-236).
  * The frame is denoised without history, as the first frame of a session (demodulate, spatial
  * variance, `settings->atrous_iterations` a-trous passes, remodulate); inputs and output are caller
@@ -411,6 +411,8 @@ typedef struct pt_server_stats {
 } pt_server_stats;
 int32_t pt_server_create(const pt_server_config* cfg, pt_server** out);
 void pt_server_destroy(pt_server* s);
+/* The message of the calling thread's last failed call on a server (the handle is shared between
+ * threads, so each thread reads its own). */
 const char* pt_server_last_error(const pt_server* s);
 /* Makes a scene resident (copied) and returns its id. PT_ERR_BUDGET when it does not fit. */
 int32_t pt_server_add_scene(pt_server* s, const pt_scene_desc* scene, int32_t* scene_id);

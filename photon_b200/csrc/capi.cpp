@@ -18,6 +18,7 @@ using namespace ptw;
 namespace {
 
 thread_local std::string g_error;
+thread_local std::string server_error;  // pt_server_last_error of the calling thread
 
 template <typename F>
 int32_t guarded(std::string* err, F&& f) {
@@ -84,7 +85,6 @@ struct pt_generated {
 
 struct pt_server {
     std::unique_ptr<Server> s;
-    std::string error;
 };
 
 extern "C" {
@@ -279,7 +279,7 @@ int32_t pt_svgf_reset(pt_svgf* s) {
 int32_t pt_svgf_run(pt_svgf* s, const float* color, const float* albedo, const float* normal_depth, const float* position,
                     const float* emission, const pt_camera* previous, const pt_svgf_settings* settings, float* output) {
     if (!s || !color || !albedo || !normal_depth || !position || !emission || !previous || !settings || !output) return PT_ERR_INVALID;
-    return guarded(&s->error, [&] {
+    return guarded(&server_error, [&] {
         PTW_CUDA(cudaSetDevice(s->device));
         s->s->run(color, albedo, normal_depth, position, emission, *previous, *settings, output);
         PTW_CUDA(cudaStreamSynchronize(s->stream));
@@ -288,7 +288,7 @@ int32_t pt_svgf_run(pt_svgf* s, const float* color, const float* albedo, const f
 
 int32_t pt_svgf_set_tma(pt_svgf* s, int32_t mode) {
     if (!s) return PT_ERR_INVALID;
-    return guarded(&s->error, [&] { s->s->set_tma(mode); });
+    return guarded(&server_error, [&] { s->s->set_tma(mode); });
 }
 
 const float* pt_svgf_variance(const pt_svgf* s) { return s ? s->s->variance() : nullptr; }
@@ -320,46 +320,47 @@ int32_t pt_server_create(const pt_server_config* cfg, pt_server** out) {
 
 void pt_server_destroy(pt_server* s) { delete s; }
 
-const char* pt_server_last_error(const pt_server* s) { return s ? s->error.c_str() : g_error.c_str(); }
+// The server handle is shared between threads, so its last error is kept per calling thread.
+const char* pt_server_last_error(const pt_server*) { return server_error.c_str(); }
 
 int32_t pt_server_add_scene(pt_server* s, const pt_scene_desc* scene, int32_t* scene_id) {
     if (!s || !scene || !scene_id) return PT_ERR_INVALID;
-    return guarded(&s->error, [&] { *scene_id = s->s->add_scene(*scene); });
+    return guarded(&server_error, [&] { *scene_id = s->s->add_scene(*scene); });
 }
 
 int32_t pt_server_submit(pt_server* s, const pt_request* req, uint64_t* request_id) {
     if (!s || !req || !request_id) return PT_ERR_INVALID;
-    return guarded(&s->error, [&] { *request_id = s->s->submit(*req); });
+    return guarded(&server_error, [&] { *request_id = s->s->submit(*req); });
 }
 
 int32_t pt_server_poll(pt_server* s, uint64_t request_id, int32_t* state) {
     if (!s || !state) return PT_ERR_INVALID;
-    return guarded(&s->error, [&] { *state = s->s->poll(request_id); });
+    return guarded(&server_error, [&] { *state = s->s->poll(request_id); });
 }
 
 int32_t pt_server_wait(pt_server* s, uint64_t request_id, double timeout_s) {
     if (!s) return PT_ERR_INVALID;
-    return guarded(&s->error, [&] { s->s->wait(request_id, timeout_s); });
+    return guarded(&server_error, [&] { s->s->wait(request_id, timeout_s); });
 }
 
 int32_t pt_server_fetch(pt_server* s, uint64_t request_id, float* rgb, size_t n, pt_request_stats* st) {
     if (!s) return PT_ERR_INVALID;
-    return guarded(&s->error, [&] { s->s->fetch(request_id, rgb, n, st); });
+    return guarded(&server_error, [&] { s->s->fetch(request_id, rgb, n, st); });
 }
 
 int32_t pt_server_cancel(pt_server* s, uint64_t request_id) {
     if (!s) return PT_ERR_INVALID;
-    return guarded(&s->error, [&] { s->s->cancel(request_id); });
+    return guarded(&server_error, [&] { s->s->cancel(request_id); });
 }
 
 int32_t pt_server_get_stats(pt_server* s, pt_server_stats* out) {
     if (!s || !out) return PT_ERR_INVALID;
-    return guarded(&s->error, [&] { s->s->stats(out); });
+    return guarded(&server_error, [&] { s->s->stats(out); });
 }
 
 int32_t pt_server_debug_fail_allocations(pt_server* s, int32_t count) {
     if (!s || count < 0) return PT_ERR_INVALID;
-    return guarded(&s->error, [&] { s->s->inject_allocation_failures(count); });
+    return guarded(&server_error, [&] { s->s->inject_allocation_failures(count); });
 }
 
 // ---- scene construction --------------------------------------------------------------------------------

@@ -123,6 +123,11 @@ int32_t Server::add_scene(const pt_scene_desc& d) {
     }
     cudaStreamDestroy(s);
     std::lock_guard<std::mutex> g(mu_);
+    // Checked again under the lock that publishes the scene: concurrent add_scene calls all passed the
+    // first check before any of them was counted, and the device scene table holds kMaxScenes entries.
+    if (int(scenes_.size()) >= kMaxScenes) throw Error{PT_ERR_BUDGET, "too many resident scenes"};
+    if (cfg_.budget_bytes && bytes_in_use_ + pool_bytes_ + scene_bytes_ + scene->device_bytes() > cfg_.budget_bytes)
+        throw Error{PT_ERR_BUDGET, "the scene does not fit the device-memory budget"};
     scene_bytes_ += scene->device_bytes();
     scenes_.push_back(std::move(scene));
     scenes_dirty_ = true;

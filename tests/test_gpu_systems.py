@@ -173,3 +173,37 @@ def test_server_cancels_running_and_queued_requests(server_scenes):
     st = s.stats()
     assert st.cancelled == 4 and st.active == 0
     s.close()
+
+
+def test_server_scene_limit_holds_under_concurrent_adds(server_scenes):
+    """add_scene from several threads at once: the scene table never grows past its 256 entries;
+    the adds beyond it fail with PT_ERR_BUDGET, and a request still renders on a scene added last."""
+    (box_desc, box_camf, box_keep), _ = server_scenes
+    srv = native.Server(budget_bytes=0, path_capacity=1 << 20)
+    ids, errors = [], []
+    lock = threading.Lock()
+
+    def add(k):
+        for _ in range(70):
+            try:
+                sid = srv.add_scene(box_desc)
+                with lock:
+                    ids.append(sid)
+            except native.PhotonError as e:
+                with lock:
+                    errors.append(e.code)
+
+    threads = [threading.Thread(target=add, args=(k,)) for k in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert len(ids) == 256 and sorted(ids) == list(range(256))
+    assert len(errors) == 4 * 70 - 256 and set(errors) == {abi.PT_ERR_BUDGET}
+    assert srv.stats().scenes == 256
+    cam = box_camf(1.0)
+    rid = srv.submit(255, cam, 32, 32, 2, seed=1)
+    srv.wait(rid, 60.0)
+    img, _ = srv.fetch(rid, 32, 32)
+    assert np.isfinite(img).all() and img.max() > 0
+    srv.close()
