@@ -322,10 +322,14 @@ void Renderer::rebuild_lights(const pt_light_update& u) {
 
 void Renderer::resize(int w, int h) {
     if (w < 0 || h < 0) throw Error{PT_ERR_INVALID, "negative image size"};
+    // Pixel indices are 32-bit in the kernels.
+    if (uint64_t(w) * uint64_t(h) > (uint64_t(1) << 30)) throw Error{PT_ERR_INVALID, "image larger than 2^30 pixels"};
     if (w == width_ && h == height_ && accum_.count) return;
     PTW_CUDA(cudaSetDevice(device_));
-    width_ = w;
-    height_ = h;
+    // No image until every buffer is sized: a failed allocation leaves a renderer that renders
+    // nothing rather than one whose buffers are smaller than its image.
+    width_ = 0;
+    height_ = 0;
     // The per-pixel buffers only grow, so a renderer that serves images of several sizes does not
     // free and allocate (each a device-wide synchronisation) on every size change. The denoiser's
     // buffers are sized on the first real-time frame.
@@ -338,6 +342,8 @@ void Renderer::resize(int w, int h) {
     display_.reserve(n);
     if (n) PTW_CUDA(cudaMemsetAsync(display_.ptr, 0, n * sizeof(uint32_t), stream_));
     PTW_CUDA(cudaStreamSynchronize(stream_));
+    width_ = w;
+    height_ = h;
     reset();
 }
 
@@ -773,19 +779,19 @@ void Renderer::render_views(const pt_view* views, int n) {
     std::vector<DevView> table(static_cast<size_t>(n));
     std::vector<int> spps(static_cast<size_t>(n));
     std::vector<uint32_t> f0(size_t(n), 0);
-    static thread_local std::vector<DeviceBuffer<float4>> pass_bufs;
-    pass_bufs.resize(size_t(n));
+    batch_pass_.resize(size_t(n));
     for (int i = 0; i < n; i++) {
         const pt_view& pv = views[i];
         if (pv.width < 0 || pv.height < 0 || pv.spp < 0) throw Error{PT_ERR_INVALID, "bad view size"};
+        if (uint64_t(pv.width) * uint64_t(pv.height) > (uint64_t(1) << 30)) throw Error{PT_ERR_INVALID, "view larger than 2^30 pixels"};
         size_t npix = size_t(pv.width) * size_t(pv.height);
         batch_accum_[size_t(i)].allocate(npix);
         batch_accum_[size_t(i)].zero(stream_);
         fill_view(table[size_t(i)], pv.camera, pv.width, pv.height, pv.spp, pv.seed, pv.path, 0);
         table[size_t(i)].accum = batch_accum_[size_t(i)].ptr;
         if (uint64_t(pv.spp) * npix > sample_cap_) {
-            pass_bufs[size_t(i)].reserve(npix);
-            table[size_t(i)].acc_pass = pass_bufs[size_t(i)].ptr;
+            batch_pass_[size_t(i)].reserve(npix);
+            table[size_t(i)].acc_pass = batch_pass_[size_t(i)].ptr;
         }
         spps[size_t(i)] = pv.spp;
     }

@@ -176,6 +176,7 @@ private:
     // batched views
     std::vector<pt_view> batch_views_;
     std::vector<DeviceBuffer<float4>> batch_accum_;
+    std::vector<DeviceBuffer<float4>> batch_pass_;   // per-view pass sums when a view is split into passes
     Counters last_ctr_{};
     pt_profile profile_{};
     cudaEvent_t acc_ev_[2] = {nullptr, nullptr};

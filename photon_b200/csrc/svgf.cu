@@ -573,8 +573,12 @@ size_t tma_buffer_elements(int w, int h) { return (size_t(h) + 9) * size_t(w) + 
 
 void SvgfDenoiser::resize(int w, int h) {
     if (w == w_ && h == h_ && illum_.ptr) return;
-    w_ = w;
-    h_ = h;
+    if (w <= 0 || h <= 0 || uint64_t(w) * uint64_t(h) > (uint64_t(1) << 30))
+        throw Error{PT_ERR_INVALID, "svgf: width and height must be positive, at most 2^30 pixels"};
+    // The size is recorded once every buffer has it, so a failed allocation cannot leave buffers
+    // smaller than the recorded frame.
+    w_ = 0;
+    h_ = 0;
     size_t n = size_t(w) * size_t(h), np = tma_buffer_elements(w, h);
     for (DeviceBuffer<float4>* b : {&prev_illum_, &prev_moments_, &prev_edge_, &illum_, &moments_}) {
         b->allocate(n);
@@ -585,6 +589,8 @@ void SvgfDenoiser::resize(int w, int h) {
         b->zero(stream_);
     }
     PTW_CUDA(cudaStreamSynchronize(stream_));
+    w_ = w;
+    h_ = h;
     has_history_ = false;
     // Tensor maps of the TMA a-trous passes over edge_, filter_[0], filter_[1]; without them (no
     // encoder in the driver, or a shape it rejects) the passes read global memory directly.

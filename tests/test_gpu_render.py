@@ -268,3 +268,24 @@ def test_adaptive_tail_is_bit_identical_alone_and_concurrent():
         t.join()
     for img in out:
         assert img is not None and np.array_equal(img, ref)
+
+
+def test_resize_rejects_oversized_images_and_keeps_working():
+    """Images beyond 2^30 pixels (32-bit pixel indices) are refused before anything is allocated;
+    the renderer keeps its previous size and renders as before."""
+    desc, camf, keep = scenes.scene("box")
+    r = native.Renderer()
+    r.upload(desc)
+    r.resize(64, 48)
+    cam = camf(64 / 48)
+    rs = abi.render_settings(64, 48, seed=2)
+    r.render(cam, rs, 2)
+    before = r.download_image()
+    with pytest.raises(native.PhotonError) as e:
+        r.resize(1 << 16, 1 << 15)
+    assert e.value.code == abi.PT_ERR_INVALID
+    assert (r.width, r.height) == (64, 48)
+    r.reset()
+    r.render(cam, rs, 2)
+    assert np.array_equal(r.download_image(), before)
+    r.close()
