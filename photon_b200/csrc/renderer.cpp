@@ -300,6 +300,10 @@ Renderer::~Renderer() {
     if (ev1_) cudaEventDestroy(ev1_);
     for (cudaEvent_t e : acc_ev_)
         if (e) cudaEventDestroy(e);
+    for (int k = 0; k < 2; k++) {
+        if (stage_ev_[k]) cudaEventDestroy(stage_ev_[k]);
+        if (stage_[k]) cudaFreeHost(stage_[k]);
+    }
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -563,23 +567,35 @@ void Renderer::download_image(float* rgb, size_t n) {
     size_t npix = size_t(width_) * size_t(height_);
     if (n < 3 * npix) throw Error{PT_ERR_INVALID, "download_image: buffer too small"};
     if (npix == 0) return;
-    std::vector<float4> raw(npix);
-    PTW_CUDA(cudaMemcpyAsync(raw.data(), denoised_ ? denoised_buf_.ptr : accum_.ptr, npix * sizeof(float4), cudaMemcpyDeviceToHost, stream_));
-    PTW_CUDA(cudaStreamSynchronize(stream_));
-    if (denoised_) {
-        for (size_t i = 0; i < npix; i++) {
-            rgb[3 * i] = raw[i].x;
-            rgb[3 * i + 1] = raw[i].y;
-            rgb[3 * i + 2] = raw[i].z;
-        }
-    } else {
-        // vec3 * (1 / samples), as GpuRenderer::download_image and CpuRenderer::image.
-        float inv = samples_ > 0 ? 1.0f / float(samples_) : 0.0f;
-        for (size_t i = 0; i < npix; i++) {
-            rgb[3 * i] = raw[i].x * inv;
-            rgb[3 * i + 1] = raw[i].y * inv;
-            rgb[3 * i + 2] = raw[i].z * inv;
-        }
+    PTW_CUDA(cudaSetDevice(device_));
+    // vec3 * (1 / samples), as GpuRenderer::download_image and CpuRenderer::image (one IEEE multiply
+    // per channel, on the device); the denoised image is copied as it is.
+    float inv = samples_ > 0 ? 1.0f / float(samples_) : 0.0f;
+    resolve_and_copy_out(denoised_ ? denoised_buf_.ptr : accum_.ptr, npix, inv, !denoised_, rgb);
+}
+
+void Renderer::resolve_and_copy_out(const float4* src, size_t npix, float scale, bool apply_scale, float* rgb) {
+    constexpr size_t kChunk = size_t(1) << 21;  // floats per pinned half (8 MiB)
+    const size_t n = 3 * npix;
+    rgb_dev_.reserve(n);
+    PTW_CUDA(wf_resolve(src, uint32_t(npix), scale, apply_scale, rgb_dev_.ptr, stream_));
+    for (int k = 0; k < 2; k++) {
+        if (!stage_[k]) PTW_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&stage_[k]), kChunk * sizeof(float), cudaHostAllocDefault));
+        if (!stage_ev_[k]) PTW_CUDA(cudaEventCreateWithFlags(&stage_ev_[k], cudaEventDisableTiming));
+    }
+    const size_t chunks = (n + kChunk - 1) / kChunk;
+    auto issue = [&](size_t c) {
+        size_t off = c * kChunk, len = std::min(kChunk, n - off);
+        PTW_CUDA(cudaMemcpyAsync(stage_[c & 1], rgb_dev_.ptr + off, len * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+        PTW_CUDA(cudaEventRecord(stage_ev_[c & 1], stream_));
+    };
+    issue(0);
+    for (size_t c = 0; c < chunks; c++) {
+        // Chunk c + 1 goes to the half that chunk c - 1 used, whose host copy has finished.
+        if (c + 1 < chunks) issue(c + 1);
+        PTW_CUDA(cudaEventSynchronize(stage_ev_[c & 1]));
+        size_t off = c * kChunk, len = std::min(kChunk, n - off);
+        std::memcpy(rgb + off, stage_[c & 1], len * sizeof(float));
     }
 }
 
@@ -821,17 +837,10 @@ void Renderer::download_view(int v, float* rgb, size_t n) {
     const pt_view& pv = batch_views_[size_t(v)];
     size_t npix = size_t(pv.width) * size_t(pv.height);
     if (n < 3 * npix) throw Error{PT_ERR_INVALID, "download_view: buffer too small"};
-    std::vector<float4> raw(npix);
-    if (npix) {
-        PTW_CUDA(cudaMemcpyAsync(raw.data(), batch_accum_[size_t(v)].ptr, npix * 16, cudaMemcpyDeviceToHost, stream_));
-        PTW_CUDA(cudaStreamSynchronize(stream_));
-    }
+    if (npix == 0) return;
+    PTW_CUDA(cudaSetDevice(device_));
     float inv = pv.spp > 0 ? 1.0f / float(pv.spp) : 0.0f;
-    for (size_t i = 0; i < npix; i++) {
-        rgb[3 * i] = raw[i].x * inv;
-        rgb[3 * i + 1] = raw[i].y * inv;
-        rgb[3 * i + 2] = raw[i].z * inv;
-    }
+    resolve_and_copy_out(batch_accum_[size_t(v)].ptr, npix, inv, true, rgb);
 }
 
 }  // namespace ptw

@@ -180,6 +180,12 @@ private:
     Counters last_ctr_{};
     pt_profile profile_{};
     cudaEvent_t acc_ev_[2] = {nullptr, nullptr};
+    // Downloads: the image resolved on the device, then copied out through two pinned halves so
+    // that the device-to-host copy of one chunk overlaps the host copy of the previous one.
+    DeviceBuffer<float> rgb_dev_;
+    float* stage_[2] = {nullptr, nullptr};
+    cudaEvent_t stage_ev_[2] = {nullptr, nullptr};
+    void resolve_and_copy_out(const float4* src, size_t npix, float scale, bool apply_scale, float* rgb);
 };
 
 }  // namespace ptw

@@ -500,7 +500,7 @@ void Server::loop() {
                     // The averaged rgb image goes into the (no longer needed) sample buffer, then to
                     // pinned host memory that fetch copies from.
                     float* rgb = reinterpret_cast<float*>(r->sample_out);
-                    PTW_CUDA(wf_resolve(r->accum, npix, 1.0f / float(r->req.spp), rgb, fin_stream_));
+                    PTW_CUDA(wf_resolve(r->accum, npix, 1.0f / float(r->req.spp), true, rgb, fin_stream_));
                     r->result_bytes = size_t(npix) * 3 * sizeof(float);
                     r->result = pinned_acquire(r->result_bytes);
                     PTW_CUDA(cudaMemcpyAsync(r->result, rgb, r->result_bytes, cudaMemcpyDeviceToHost, fin_stream_));

@@ -11,6 +11,7 @@
 
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "gbuffer.cuh"
 #include "pt_math.cuh"
@@ -622,12 +623,21 @@ void SvgfDenoiser::build_tma_plan() {
     if (tma_mode_ == 0 || w_ == 0) return;
     PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
     if (!encode) return;
-    static std::once_flag attr_once;
-    std::call_once(attr_once, [] {
+    {
+        // Kernel attributes belong to a device: set them once on each device that runs the passes.
         // Up to 2 x 48 x 48 float4 of tiles (contiguous, step 8) per block.
-        cudaFuncSetAttribute(k_atrous_tma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem_bytes(8)));
-        cudaFuncSetAttribute(k_atrous_tma<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem_bytes(8)));
-    });
+        static std::mutex attr_mu;
+        static std::vector<int> attr_done;
+        int dev = 0;
+        PTW_CUDA(cudaGetDevice(&dev));
+        std::lock_guard<std::mutex> g(attr_mu);
+        if (size_t(dev) >= attr_done.size()) attr_done.resize(size_t(dev) + 1, 0);
+        if (!attr_done[size_t(dev)]) {
+            PTW_CUDA(cudaFuncSetAttribute(k_atrous_tma<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem_bytes(8))));
+            PTW_CUDA(cudaFuncSetAttribute(k_atrous_tma<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem_bytes(8))));
+            attr_done[size_t(dev)] = 1;
+        }
+    }
     float4* bufs[3] = {edge_.ptr, filter_[0].ptr, filter_[1].ptr};
     const int w = w_, h = h_;
     for (int b = 0; b < 3; b++)

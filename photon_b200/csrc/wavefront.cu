@@ -820,8 +820,6 @@ __global__ void k_display(DisplayParams p, const float4* accum, const float4* de
     out[i] = pack_rgba8_d(c);
 }
 
-int g_smem_trace = 0;
-
 }  // namespace
 
 cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, LaunchShape* out) {
@@ -857,7 +855,6 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade, shade_block, 0);
     if (e != cudaSuccess) return e;
     out->shade_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
-    g_smem_trace = int(smem);
     return cudaSuccess;
 }
 
@@ -921,18 +918,23 @@ cudaError_t wf_iteration(const WfParams& p, const LaunchShape& ls, cudaStream_t 
     return cudaGetLastError();
 }
 
-__global__ void k_resolve(const float4* __restrict__ accum, uint32_t n, float scale, float* __restrict__ rgb) {
+__global__ void k_resolve(const float4* __restrict__ accum, uint32_t n, float scale, int apply_scale, float* __restrict__ rgb) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4 a = accum[i];
-    rgb[3 * size_t(i)] = a.x * scale;
-    rgb[3 * size_t(i) + 1] = a.y * scale;
-    rgb[3 * size_t(i) + 2] = a.z * scale;
+    if (apply_scale) {
+        a.x = a.x * scale;
+        a.y = a.y * scale;
+        a.z = a.z * scale;
+    }
+    rgb[3 * size_t(i)] = a.x;
+    rgb[3 * size_t(i) + 1] = a.y;
+    rgb[3 * size_t(i) + 2] = a.z;
 }
 
-cudaError_t wf_resolve(const float4* accum, uint32_t n, float scale, float* rgb, cudaStream_t stream) {
+cudaError_t wf_resolve(const float4* accum, uint32_t n, float scale, bool apply_scale, float* rgb, cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
-    k_resolve<<<(n + 255) / 256, 256, 0, stream>>>(accum, n, scale, rgb);
+    k_resolve<<<(n + 255) / 256, 256, 0, stream>>>(accum, n, scale, apply_scale ? 1 : 0, rgb);
     return cudaGetLastError();
 }
 

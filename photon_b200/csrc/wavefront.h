@@ -112,7 +112,8 @@ constexpr int kKernelsPerIteration = 5;
 // Sums the samples of every pixel of a view in sample order (after a pass).
 cudaError_t wf_accumulate(const DevView* d_view, const DevView& h_view, int first_pass, int last_pass, cudaStream_t stream);
 // rgb[3 i + c] = accum[i].c * scale for n pixels (a finished image, averaged over its samples).
-cudaError_t wf_resolve(const float4* accum, uint32_t n, float scale, float* rgb, cudaStream_t stream);
+// rgb[3i..3i+2] = accum[i].xyz * scale (or the plain xyz when apply_scale is false).
+cudaError_t wf_resolve(const float4* accum, uint32_t n, float scale, bool apply_scale, float* rgb, cudaStream_t stream);
 
 // Probes (same device functions as the wavefront).
 cudaError_t wf_trace_primary(const DevScene* scene, const float* cam16, int w, int h, uint32_t frame, uint32_t seed,

@@ -198,9 +198,14 @@ class Renderer:
     def last_frame_ms(self):
         return self.stats().last_frame_ms
 
-    def download_image(self):
+    def download_image(self, out=None):
+        """The image (height, width, 3) float32; `out`, a C-contiguous float32 array of that shape, is
+        filled in place when given (a reused host buffer)."""
         s = self.stats()
-        out = np.zeros((s.height, s.width, 3), np.float32)
+        if out is None:
+            out = np.zeros((s.height, s.width, 3), np.float32)
+        elif out.dtype != np.float32 or out.shape != (s.height, s.width, 3) or not out.flags.c_contiguous:
+            raise ValueError("download_image: out must be a C-contiguous float32 array of shape (height, width, 3)")
         _check(lib.pt_download_image(self.h, out, out.size), self._err)
         return out
 
