@@ -145,11 +145,10 @@ __global__ void __launch_bounds__(256) k_generate(const __grid_constant__ WfPara
     Counters* c = P.ctr;
     const uint32_t p = c->parity, base = c->gen_base, n = c->gen_n;
     const unsigned long long wb = c->work_base;
-    for (;;) {
-        uint32_t k0 = warp_fetch(&c->fetch[0]);
-        if (k0 >= n) break;
-        uint32_t k = k0 + lane_id();
-        if (k >= n) continue;
+    // Every path costs the same here, so a static grid-stride split replaces the claim counter: one
+    // atomic per warp on one address held this kernel at 1.5 ms per 1080p frame (0.56 ms without).
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
         unsigned long long wg = wb + k;
         const int v0 = int(c->gen_view);
         int vi = v0 + find_view(P.views + v0, P.num_views - v0, wg);
