@@ -235,6 +235,7 @@ void WavefrontEngine::begin(const DevScene* scenes, const DevView* views, int n_
     std::memset(h_ctr_, 0, sizeof(Counters));
     h_ctr_->parity = 1;
     h_ctr_->tail_limit = tail_limit(tuning_.tail_paths, false);  // a server shares the GPU between requests
+    tail_limit_ = h_ctr_->tail_limit;
     PTW_CUDA(cudaMemcpyAsync(ctr_.ptr, h_ctr_, sizeof(Counters), cudaMemcpyHostToDevice, stream_));
     cont_params_ = params(scenes, -1, views, n_views, false);
 }

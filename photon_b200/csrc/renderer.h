@@ -69,6 +69,9 @@ public:
     // from its own staging memory (set_work_total_async).
     void launch(int iterations);
     Counters* device_counters() const { return ctr_.ptr; }
+    // Queued paths at or below which an iteration hands everything to the tail (0: never), as set by
+    // the last begin().
+    uint32_t tail_limit_in_use() const { return tail_limit_; }
     void set_work_total_async(const unsigned long long* pinned_value);
 
     const Counters& last() const { return last_; }
@@ -110,6 +113,7 @@ private:
     WfParams cont_params_{};
     int profile_flags_ = 0;
     std::vector<cudaEvent_t> prof_ev_;
+    uint32_t tail_limit_ = 0;
     void collect_kernel_times(int iterations);
 };
 

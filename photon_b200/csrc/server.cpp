@@ -461,7 +461,12 @@ void Server::loop() {
 
             // Launch this batch, then read the previous one's results while it runs.
             if (launch) {
-                B.iterations = iters_per_batch_;
+                // Work not yet generated plus paths queued can only shrink between batches (apart from
+                // new chunks, counted in work_total_), so if even this stale count fits the tail,
+                // the next iteration finishes everything and the rest of a batch would be empty.
+                const uint64_t pending = (work_total_ - generated_) + queued_;
+                const uint32_t tail = engine_->tail_limit_in_use();
+                B.iterations = (tail > 0 && pending <= tail) ? 1 : iters_per_batch_;
                 PTW_CUDA(cudaEventRecord(B.ev_start, stream_));
                 engine_->launch(B.iterations);
                 PTW_CUDA(cudaMemcpyAsync(B.ctr, engine_->device_counters(), sizeof(Counters), cudaMemcpyDeviceToHost, stream_));
@@ -475,6 +480,7 @@ void Server::loop() {
                 PTW_CUDA(cudaEventSynchronize(P.ev));
                 P.in_flight = false;
                 generated_ = P.ctr->work_next;
+                queued_ = P.ctr->count[P.ctr->parity ^ 1u];
                 iterations_ = P.ctr->iterations;
                 // Aim for batches of about a millisecond of device time: long enough that the host's
                 // turn between batches stays hidden, short enough that finished requests and new

@@ -115,6 +115,7 @@ private:
     int iters_per_batch_ = 2;  // adapted so that a batch keeps the device busy for about a millisecond
     cudaStream_t fin_stream_ = nullptr;
     uint64_t generated_ = 0;       // work items generated, as of the last completed batch
+    uint64_t queued_ = 0;          // paths queued for the next iteration, as of the last completed batch
     uint64_t iterations_ = 0;
     size_t views_uploaded_ = 0;
     uint64_t work_total_ = 0;
