@@ -165,7 +165,7 @@ uint64_t Server::submit(const pt_request& r) {
 int32_t Server::poll(uint64_t id) {
     std::lock_guard<std::mutex> g(mu_);
     auto it = requests_.find(id);
-    if (it == requests_.end()) throw Error{PT_ERR_NOT_FOUND, "unknown request"};
+    if (it == requests_.end() || it->second->fetched) throw Error{PT_ERR_NOT_FOUND, "unknown request"};
     return it->second->state;
 }
 
@@ -175,7 +175,7 @@ void Server::wait(uint64_t id, double timeout_s) {
                                                             std::chrono::duration<double>(std::max(0.0, timeout_s)));
     for (;;) {
         auto it = requests_.find(id);
-        if (it == requests_.end()) throw Error{PT_ERR_NOT_FOUND, "unknown request"};
+        if (it == requests_.end() || it->second->fetched) throw Error{PT_ERR_NOT_FOUND, "unknown request"};
         int s = it->second->state;
         if (s == PT_REQ_DONE) return;
         if (s == PT_REQ_CANCELLED) throw Error{PT_ERR_CANCELLED, "request cancelled"};
@@ -191,7 +191,7 @@ void Server::wait(uint64_t id, double timeout_s) {
 void Server::fetch(uint64_t id, float* rgb, size_t n, pt_request_stats* st) {
     std::lock_guard<std::mutex> g(mu_);
     auto it = requests_.find(id);
-    if (it == requests_.end()) throw Error{PT_ERR_NOT_FOUND, "unknown request"};
+    if (it == requests_.end() || it->second->fetched) throw Error{PT_ERR_NOT_FOUND, "unknown request"};
     Request& r = *it->second;
     if (r.state == PT_REQ_QUEUED || r.state == PT_REQ_RUNNING) throw Error{PT_ERR_INVALID, "request not finished"};
     if (st) {
@@ -208,14 +208,15 @@ void Server::fetch(uint64_t id, float* rgb, size_t n, pt_request_stats* st) {
     int state = r.state;
     pinned_release(r.result, r.result_bytes);
     r.result = nullptr;
-    requests_.erase(it);
+    r.fetched = true;
+    if (r.batch_refs == 0) requests_.erase(it);  // else the loop erases it after its last batch
     if (state == PT_REQ_CANCELLED) throw Error{PT_ERR_CANCELLED, "request cancelled"};
 }
 
 void Server::cancel(uint64_t id) {
     std::lock_guard<std::mutex> g(mu_);
     auto it = requests_.find(id);
-    if (it == requests_.end()) throw Error{PT_ERR_NOT_FOUND, "unknown request"};
+    if (it == requests_.end() || it->second->fetched) throw Error{PT_ERR_NOT_FOUND, "unknown request"};
     Request& r = *it->second;
     if (r.state == PT_REQ_QUEUED) {
         queue_.erase(std::remove(queue_.begin(), queue_.end(), id), queue_.end());
@@ -242,6 +243,14 @@ void Server::stats(pt_server_stats* out) {
 void Server::inject_allocation_failures(int n) {
     std::lock_guard<std::mutex> g(mu_);
     inject_failures_ = n;
+}
+
+// Called with the lock held: drops the references of a completed batch's snapshot, erasing the
+// requests that were fetched meanwhile.
+void Server::release_batch_refs(const std::vector<Request*>& reqs) {
+    for (Request* r : reqs) {
+        if (--r->batch_refs == 0 && r->fetched) requests_.erase(r->id);
+    }
 }
 
 void Server::upload_scene_table() {
@@ -443,6 +452,7 @@ void Server::loop() {
             size_t lo = size_t(done_slots_), hi = 0;
             for (uint64_t id : active_) {
                 Request* r = requests_[id].get();
+                r->batch_refs++;
                 B.reqs.push_back(r);
                 B.need.push_back(r->cancel ? r->appended : r->work);
                 lo = std::min(lo, size_t(r->done_slot));
@@ -475,7 +485,7 @@ void Server::loop() {
                 PTW_CUDA(cudaEventRecord(B.ev, stream_));
                 B.in_flight = true;
             }
-            std::vector<Request*> finished, cancelled;
+            std::vector<Request*> finished, cancelled, released;
             if (P.in_flight) {
                 PTW_CUDA(cudaEventSynchronize(P.ev));
                 P.in_flight = false;
@@ -517,6 +527,8 @@ void Server::loop() {
                     finishing_.push_back(f);
                 }
                 for (Request* r : cancelled) release_buffers(*r, stream_);
+                released = std::move(P.reqs);
+                P.reqs.clear();
             }
             // Images whose copy has landed: normalise by the sample count. With nothing else to do,
             // wait for the oldest copy instead of polling.
@@ -555,13 +567,18 @@ void Server::loop() {
                 st_.samples_done += r->work;
             }
             if (!done.empty() || !cancelled.empty()) cv_done_.notify_all();
+            release_batch_refs(released);
             cur ^= 1;
         } catch (const Error& e) {
             if (!lk.owns_lock()) lk.lock();
             cudaStreamSynchronize(stream_);
             cudaStreamSynchronize(fin_stream_);
             cudaGetLastError();
-            for (Batch& b : batch_) b.in_flight = false;
+            for (Batch& b : batch_) {
+                b.in_flight = false;
+                release_batch_refs(b.reqs);
+                b.reqs.clear();
+            }
             for (Finishing& f : finishing_) {
                 cudaEventDestroy(f.ev);
                 f.r->state = PT_REQ_FAILED;

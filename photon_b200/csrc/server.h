@@ -46,6 +46,10 @@ private:
         DevView tmpl{};         // the view of the whole image; chunks differ in work range only
         std::atomic<bool> cancel{false};
         bool finishing = false;  // its image is being summed and copied out
+        // Batches whose snapshot lists this request. A fetched request is erased only once none
+        // does, since the loop reads a batch's requests after the batch completes, without the lock.
+        int batch_refs = 0;
+        bool fetched = false;
         std::string error;
         float4* sample_out = nullptr;  // stream-ordered allocations from the server's memory pool
         float4* accum = nullptr;
@@ -62,6 +66,7 @@ private:
     float* pinned_acquire(size_t bytes);
     void pinned_release(float* p, size_t bytes);
     void upload_scene_table();
+    void release_batch_refs(const std::vector<Request*>& reqs);
 
     pt_server_config cfg_;
     int device_;

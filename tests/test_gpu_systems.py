@@ -207,3 +207,45 @@ def test_server_scene_limit_holds_under_concurrent_adds(server_scenes):
     img, _ = srv.fetch(rid, 32, 32)
     assert np.isfinite(img).all() and img.max() > 0
     srv.close()
+
+
+def test_server_survives_immediate_fetches_of_many_small_requests(server_scenes):
+    """Many tiny requests from several threads, each fetched the moment it is done: a fetched
+    request may still be listed by a batch that the server has not read back yet, so the server must
+    keep it until then (it did not, and read freed memory). Every image arrives and equals the same
+    request rendered alone."""
+    (box_desc, box_camf, box_keep), _ = server_scenes
+    srv = native.Server(budget_bytes=0, path_capacity=1 << 20)
+    sid = srv.add_scene(box_desc)
+    cam = box_camf(1.0)
+    failures = []
+
+    def client(k):
+        try:
+            for j in range(60):
+                rid = srv.submit(sid, cam, 16, 16, 1, seed=100 * k + j)
+                srv.wait(rid, 60.0)
+                img, st = srv.fetch(rid, 16, 16)
+                if not np.isfinite(img).all():
+                    failures.append((k, j, "not finite"))
+                with pytest.raises(native.PhotonError):
+                    srv.poll(rid)
+        except Exception as e:  # noqa: BLE001 - reported below
+            failures.append((k, repr(e)))
+
+    threads = [threading.Thread(target=client, args=(k,)) for k in range(6)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not failures, failures[:3]
+    rid = srv.submit(sid, cam, 16, 16, 1, seed=205)
+    srv.wait(rid, 60.0)
+    served, _ = srv.fetch(rid, 16, 16)
+    srv.close()
+    r = native.Renderer()
+    r.upload(box_desc)
+    r.resize(16, 16)
+    r.render(cam, abi.RenderSettings(16, 16, abi.path_options(), 1.0, abi.PT_TONEMAP_ACES, 205), 1)
+    assert np.array_equal(served.view(np.uint32), r.download_image().view(np.uint32))
+    r.close()
