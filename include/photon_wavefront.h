@@ -385,7 +385,7 @@ typedef struct pt_server_config {
     int32_t device;
     uint64_t budget_bytes;     /* device memory for scenes + requests + path pool */
     int32_t path_capacity;     /* shared path pool (0: 8,388,608 paths) */
-    int32_t max_active;        /* requests on the device at once (0: unbounded, budget only) */
+    int32_t max_active;        /* requests on the device at once (0: 16; negative: unbounded, budget only) */
     double device_wait_seconds;/* bound of every device-side wait (0: 2 s) */
 } pt_server_config;
 typedef struct pt_request {
