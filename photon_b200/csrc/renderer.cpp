@@ -220,7 +220,7 @@ void WavefrontEngine::run(const DevScene* scenes, int single_scene, const DevVie
         }
         PTW_CUDA(cudaEventRecord(ev_, stream_));
         PTW_CUDA(cudaEventSynchronize(ev_));
-        kernel_launches += uint64_t(iters) * kKernelsPerIteration;
+        kernel_launches += uint64_t(iters) * uint64_t(wf_kernels_per_iteration(p));
         iteration_launches += uint64_t(iters);
         if (timed) collect_kernel_times(iters);
         const Counters& h = *h_ctr_;
@@ -258,14 +258,14 @@ void WavefrontEngine::append_work(uint64_t new_total) {
 
 void WavefrontEngine::iterate(int iterations) {
     for (int k = 0; k < iterations; k++) PTW_CUDA(wf_iteration(cont_params_, shape_, stream_));
-    kernel_launches += uint64_t(iterations) * kKernelsPerIteration;
+    kernel_launches += uint64_t(iterations) * uint64_t(wf_kernels_per_iteration(cont_params_));
     iteration_launches += uint64_t(iterations);
     PTW_CUDA(cudaMemcpyAsync(h_ctr_, ctr_.ptr, sizeof(Counters), cudaMemcpyDeviceToHost, stream_));
 }
 
 void WavefrontEngine::launch(int iterations) {
     for (int k = 0; k < iterations; k++) PTW_CUDA(wf_iteration(cont_params_, shape_, stream_));
-    kernel_launches += uint64_t(iterations) * kKernelsPerIteration;
+    kernel_launches += uint64_t(iterations) * uint64_t(wf_kernels_per_iteration(cont_params_));
     iteration_launches += uint64_t(iterations);
 }
 

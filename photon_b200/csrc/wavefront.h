@@ -105,10 +105,12 @@ struct LaunchShape {
 
 // Fills grid sizes from the occupancy of each kernel on `device` (block sizes as requested).
 cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, LaunchShape* out);
-// One bounce iteration: setup, generate, trace, shade, shadow. With `events` (6 entries), an event
-// is recorded before the first kernel and after each of the five.
+// One bounce iteration: setup, generate, [tail], trace, shade, shadow [, the three ray-sort kernels].
+// With `events` (6 entries), an event is recorded before the first kernel and after each of the five
+// stages (the tail counts with trace, the sort kernels with shadow).
 cudaError_t wf_iteration(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, cudaEvent_t* events = nullptr);
-constexpr int kKernelsPerIteration = 5;
+// Kernels wf_iteration launches for these parameters.
+inline int wf_kernels_per_iteration(const WfParams& p) { return 5 + (p.tail_paths > 0 ? 1 : 0) + (p.sort_bits > 0 ? 3 : 0); }
 // Sums the samples of every pixel of a view in sample order (after a pass).
 cudaError_t wf_accumulate(const DevView* d_view, const DevView& h_view, int first_pass, int last_pass, cudaStream_t stream);
 // rgb[3 i + c] = accum[i].c * scale for n pixels (a finished image, averaged over its samples).
