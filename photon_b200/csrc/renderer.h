@@ -31,7 +31,8 @@ struct Tuning {
     int shade_block = 256;
     int sort_by_material = 4;      // shade windows of 4 x shade_block paths grouped by material class
     int graph_bounces = 4;         // iterations per CUDA graph launch
-    int sort_rays = 0;             // origin bits per axis of the ray-sort key (0: no sorting)
+    int sort_rays = 4;             // origin bits per axis of the ray-sort key (0: no sorting); iterations of
+                                   // at least 2M paths only
     int packed = 1;                // f32x2 slab tests
     int wide_shadows = 0;          // 1: shadow rays walk the 4-wide BVH (measured slower on the 262K scene)
     int tail_paths = kTailAuto;    // finish the last queued paths one thread each below this many (0: never)

@@ -110,6 +110,8 @@ __device__ __forceinline__ int find_view(const DevView* views, int n, unsigned l
     return lo;
 }
 
+constexpr uint32_t kSortMinPaths = 1u << 21;  // iterations with fewer paths are not ray-sorted
+
 // ---- setup ------------------------------------------------------------------------------------------
 __global__ void k_setup(const __grid_constant__ WfParams P) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -136,6 +138,8 @@ __global__ void k_setup(const __grid_constant__ WfParams P) {
     c->shadow_count = 0;
     c->rays += cnt + n;
     c->tail = (tail_paths > 0 && cnt + n > 0 && cnt + n <= tail_paths && c->work_next >= c->work_total) ? 1u : 0u;
+    // Sorting pays for its scan and scatter only on large iterations.
+    c->sorting = (P.sort_bits > 0 && !c->tail && cnt + n >= kSortMinPaths) ? 1u : 0u;
     for (int k = 0; k < 6; k++) c->fetch[k] = 0;
     if (cnt + n > 0) c->iterations++;
 }
@@ -381,7 +385,7 @@ __device__ __forceinline__ void shade_path(const WfParams& P, Counters* c, uint3
     const uint4 id = st.id;
     // Continuing paths move to the other buffer, compacted.
     uint32_t slot = warp_append(cont, &c->count[q]);
-    if (P.sort_bits > 0) {
+    if (P.sort_bits > 0 && c->sorting) {
         uint32_t key = cont ? ray_key(scene_for(P, id.x), st.ro, st.rd, P.sort_bits) : 0xffffffffu;
         uint32_t peers = __match_any_sync(kFull, key);
         if (cont) {
@@ -590,6 +594,7 @@ __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfPar
 // ---- ray sorting: a counting sort of the shade output by ray key ------------------------------------------
 // Exclusive scan of the bucket counts into write offsets (one block), then zero the counts.
 __global__ void __launch_bounds__(1024) k_sort_scan(const __grid_constant__ WfParams P, uint32_t buckets) {
+    if (!P.ctr->sorting) return;
     __shared__ uint32_t part[1024];
     uint32_t per = (buckets + 1023) / 1024;
     uint32_t lo = threadIdx.x * per, hi = min(lo + per, buckets);
@@ -616,10 +621,11 @@ __global__ void __launch_bounds__(1024) k_sort_scan(const __grid_constant__ WfPa
 // bucket's next position; the next setup then finds the sorted paths there.
 __global__ void __launch_bounds__(256) k_sort_scatter(const __grid_constant__ WfParams P) {
     Counters* c = P.ctr;
+    if (!c->sorting) return;
     const uint32_t p = c->parity, q = p ^ 1u, n = c->count[q];
-    for (;;) {
-        uint32_t i0 = warp_fetch(&c->fetch[4]);
-        if (i0 >= n) break;
+    // Whole warps over consecutive runs of 32 paths, split statically (no claim counter).
+    const uint32_t warps = gridDim.x * (blockDim.x / 32u);
+    for (uint32_t i0 = (blockIdx.x * (blockDim.x / 32u) + threadIdx.x / 32u) * 32u; i0 < n; i0 += warps * 32u) {
         uint32_t i = i0 + lane_id();
         uint32_t key = i < n ? P.keys[i] : 0xffffffffu;
         uint32_t peers = __match_any_sync(kFull, key);
@@ -640,7 +646,7 @@ __global__ void __launch_bounds__(256) k_sort_scatter(const __grid_constant__ Wf
 
 // After the scatter: the sorted paths live in the input buffer; make the next setup flip to it.
 __global__ void k_sort_finish(Counters* c) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (threadIdx.x != 0 || blockIdx.x != 0 || !c->sorting) return;
     uint32_t p = c->parity, q = p ^ 1u;
     c->count[p] = c->count[q];
     c->count[q] = 0;

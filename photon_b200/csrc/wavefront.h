@@ -49,6 +49,7 @@ struct Counters {
     uint32_t overflow;
     uint32_t tail;                   // 1: this iteration finishes every queued path in k_tail
     uint32_t tail_limit;             // queued paths at or below which k_tail takes over (host-set per render)
+    uint32_t sorting;                // 1: this iteration's continuing rays are sorted (sort_bits > 0, enough paths)
     uint32_t gen_view;               // first view whose work is not all generated (views are in work order)
     uint32_t iterations;
     unsigned long long work_base, work_next, work_total;
