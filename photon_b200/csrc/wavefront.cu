@@ -592,28 +592,48 @@ __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfPar
 }
 
 // ---- ray sorting: a counting sort of the shade output by ray key ------------------------------------------
-// Exclusive scan of the bucket counts into write offsets (one block), then zero the counts.
+// Exclusive scan of the bucket counts into write offsets (one block), then zero the counts. Each warp
+// takes a contiguous 32nd of the buckets and reads it 32 consecutive counts at a time (coalesced):
+// a first pass sums its part, the 32 part sums are scanned, and a second pass writes the offsets.
 __global__ void __launch_bounds__(1024) k_sort_scan(const __grid_constant__ WfParams P, uint32_t buckets) {
     if (!P.ctr->sorting) return;
-    __shared__ uint32_t part[1024];
-    uint32_t per = (buckets + 1023) / 1024;
-    uint32_t lo = threadIdx.x * per, hi = min(lo + per, buckets);
-    uint32_t sum = 0;
-    for (uint32_t k = lo; k < hi; k++) sum += P.hist[k];
-    part[threadIdx.x] = sum;
-    __syncthreads();
-    for (uint32_t off = 1; off < 1024; off <<= 1) {
-        uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
-        __syncthreads();
-        part[threadIdx.x] += v;
-        __syncthreads();
+    __shared__ uint32_t part[32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t per = (buckets + 31u) / 32u;
+    const uint32_t lo = min(warp * per, buckets), hi = min(lo + per, buckets);
+    uint32_t total = 0;
+    for (uint32_t base = lo; base < hi; base += 32u) {
+        const uint32_t k = base + lane;
+        uint32_t v = k < hi ? P.hist[k] : 0u;
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
+        total += v;
     }
-    uint32_t run = part[threadIdx.x] - sum;  // exclusive prefix of this thread's range
-    for (uint32_t k = lo; k < hi; k++) {
-        uint32_t h = P.hist[k];
-        P.offsets[k] = run;
-        run += h;
-        P.hist[k] = 0;
+    if (lane == 0) part[warp] = total;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t t = part[lane];
+        uint32_t incl = t;
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t v = __shfl_up_sync(kFull, incl, off);
+            if (int(lane) >= off) incl += v;
+        }
+        part[lane] = incl - t;
+    }
+    __syncthreads();
+    uint32_t carry = part[warp];
+    for (uint32_t base = lo; base < hi; base += 32u) {
+        const uint32_t k = base + lane;
+        const uint32_t v = k < hi ? P.hist[k] : 0u;
+        uint32_t incl = v;
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t u = __shfl_up_sync(kFull, incl, off);
+            if (int(lane) >= off) incl += u;
+        }
+        if (k < hi) {
+            P.offsets[k] = carry + incl - v;
+            P.hist[k] = 0;
+        }
+        carry += __shfl_sync(kFull, incl, 31);
     }
 }
 
