@@ -206,6 +206,8 @@ void WavefrontEngine::run(const DevScene* scenes, int single_scene, const DevVie
     h_ctr_->tail_limit = tail_limit(tuning_.tail_paths, busy.others == 0);
     PTW_CUDA(cudaMemcpyAsync(ctr_.ptr, h_ctr_, sizeof(Counters), cudaMemcpyHostToDevice, stream_));
     WfParams p = params(scenes, single_scene, views, n_views, count_work || (profile_flags_ & PT_PROFILE_TRAVERSAL_COUNTS));
+    // A render too small for any iteration to reach the sorting threshold launches no sort kernels.
+    if (std::min<uint64_t>(total_work, uint64_t(tuning_.path_capacity)) < kSortMinPaths) p.sort_bits = 0;
     bool use_graph = tuning_.graph_bounces > 0;
     bool timed = (profile_flags_ & PT_PROFILE_KERNEL_TIMES) != 0;
     if (use_graph && (!graph_ || std::memcmp(&graph_params_, &p, sizeof(p)) != 0 || graph_iters_ != tuning_.graph_bounces)) capture(p);

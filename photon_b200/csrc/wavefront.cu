@@ -110,8 +110,6 @@ __device__ __forceinline__ int find_view(const DevView* views, int n, unsigned l
     return lo;
 }
 
-constexpr uint32_t kSortMinPaths = 1u << 21;  // iterations with fewer paths are not ray-sorted
-
 // ---- setup ------------------------------------------------------------------------------------------
 __global__ void k_setup(const __grid_constant__ WfParams P) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;

@@ -110,6 +110,9 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
 // With `events` (6 entries), an event is recorded before the first kernel and after each of the five
 // stages (the tail counts with trace, the sort kernels with shadow).
 cudaError_t wf_iteration(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, cudaEvent_t* events = nullptr);
+// Iterations with fewer queued paths are not ray-sorted (the scan and scatter would cost more than the
+// coherence gains).
+constexpr uint32_t kSortMinPaths = 1u << 21;
 // Kernels wf_iteration launches for these parameters.
 inline int wf_kernels_per_iteration(const WfParams& p) { return 5 + (p.tail_paths > 0 ? 1 : 0) + (p.sort_bits > 0 ? 3 : 0); }
 // Sums the samples of every pixel of a view in sample order (after a pass).
