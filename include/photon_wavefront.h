@@ -237,7 +237,7 @@ typedef struct pt_tuning {
     int32_t sort_by_material;  /* k in 1-4: the shading kernel groups windows of k x shade_block paths by material
                                   class before shading them; 0: queue order; -1 keep */
     int32_t graph_bounces;     /* bounce iterations captured per CUDA graph launch */
-    int32_t sort_rays;         /* 0 off, 1-4: sort continuing rays by direction octant + Morton origin cell
+    int32_t sort_rays;         /* 0 off, 1-6: sort continuing rays by direction octant + Morton origin cell
                                   with this many bits per axis before tracing them, on iterations of at
                                   least 2,097,152 paths (4: the renderer's default; the server: 0); -1 keep */
     int32_t packed;            /* 1: f32x2 (packed FP32) slab tests in traversal, 0: scalar; -1 keep */

@@ -668,7 +668,7 @@ void Renderer::set_tuning(const pt_tuning& t) {
     }
     if (t.graph_bounces >= 0) cur.graph_bounces = t.graph_bounces;
     if (t.sort_rays >= 0) {
-        if (t.sort_rays > 4) throw Error{PT_ERR_INVALID, "sort_rays must be in [0, 4]"};
+        if (t.sort_rays > 6) throw Error{PT_ERR_INVALID, "sort_rays must be in [0, 6]"};
         cur.sort_rays = t.sort_rays;
     }
     if (t.packed >= 0) cur.packed = t.packed ? 1 : 0;
@@ -743,7 +743,7 @@ void Renderer::autotune(const pt_camera& cam, const pt_render_settings& rs, int 
     try_knob([](Tuning& t, int v) { t.shade_block = v; }, {64, 128, 256});
     try_knob([](Tuning& t, int v) { t.sort_by_material = v; }, {0, 1, 2, 4});
     try_knob([](Tuning& t, int v) { t.graph_bounces = v; }, {2, 4, 8});
-    try_knob([](Tuning& t, int v) { t.sort_rays = v; }, {0, 3});
+    try_knob([](Tuning& t, int v) { t.sort_rays = v; }, {0, 3, 4, 5});
     try_knob([](Tuning& t, int v) { t.tail_paths = v; }, {0, 1 << 16, 1 << 17, 1 << 18, 1 << 20});
     try_knob([](Tuning& t, int v) { t.wide_shadows = v; }, {0, 1});
     engine_->set_tuning(best);
