@@ -291,7 +291,7 @@ def test_resize_rejects_oversized_images_and_keeps_working():
     r.close()
 
 
-@pytest.mark.parametrize("bits", [3, 4])
+@pytest.mark.parametrize("bits", [3, 4, 5])
 def test_ray_sorting_is_bit_identical(bits):
     """Ray sorting runs only on iterations of at least 2^20 paths (smaller ones do not pay for the
     scan and scatter): a 512x288x8 frame (1.18 M paths) sorts its first bounces, and its image equals
