@@ -435,8 +435,11 @@ __device__ __forceinline__ uint32_t shade_key(const WfParams& P, uint32_t p, uin
 // shared memory (a counting sort on 64 keys) and shades them in that order, so a warp mostly runs one
 // BSDF lobe and one texture pattern. The order in which paths are shaded changes only where their
 // outputs are appended, not any path's result.
-constexpr int kMaxShadeRounds = 4;  // sort_material <= 4 and window <= 1024 paths
-constexpr uint32_t kMaxShadeWindow = 1024;
+// On iterations whose continuing rays are sorted afterwards (Counters::sorting), the order of the
+// shade output no longer matters to the next trace, so the window grows fourfold (16 x 256 paths)
+// for more coherent shading.
+constexpr uint32_t kMaxShadeRounds = 16;
+constexpr uint32_t kMaxShadeWindow = kMaxShadeRounds * 256;
 __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ WfParams P) {
     Counters* c = P.ctr;
     if (c->tail) return;
@@ -450,21 +453,31 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ WfParams 
         }
         return;
     }
-    __shared__ uint32_t s_base, s_hist[kShadeKeys], s_perm[kMaxShadeWindow];
-    const uint32_t tid = threadIdx.x, window = uint32_t(P.sort_material) * blockDim.x;
+    __shared__ uint32_t s_base, s_hist[kShadeKeys], s_perm[kMaxShadeWindow], s_kr[kMaxShadeWindow];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t rounds = min(uint32_t(P.sort_material) * (c->sorting ? 4u : 1u), kMaxShadeRounds);
+    const uint32_t window = rounds * blockDim.x;
     for (;;) {
         if (tid == 0) s_base = atomicAdd(&c->fetch[2], window);
         for (uint32_t k = tid; k < kShadeKeys; k += blockDim.x) s_hist[k] = 0;
         __syncthreads();
         const uint32_t i0 = s_base;
         if (i0 >= n) break;
-        uint32_t key[kMaxShadeRounds], rank[kMaxShadeRounds];
+        // Keys four rounds at a time (their dependent loads overlap), kept with their ranks in
+        // shared memory as key << 16 | rank.
+        for (uint32_t r0 = 0; r0 < rounds; r0 += 4) {
+            uint32_t key[4];
 #pragma unroll
-        for (int r = 0; r < kMaxShadeRounds; r++) {
-            if (r < P.sort_material) {
-                const uint32_t i = i0 + uint32_t(r) * blockDim.x + tid;
-                key[r] = i < n ? shade_key(P, p, i) : kShadeKeys - 1;
-                rank[r] = atomicAdd(&s_hist[key[r]], 1u);
+            for (uint32_t q = 0; q < 4; q++) {
+                const uint32_t i = i0 + (r0 + q) * blockDim.x + tid;
+                key[q] = (r0 + q < rounds && i < n) ? shade_key(P, p, i) : kShadeKeys - 1;
+            }
+#pragma unroll
+            for (uint32_t q = 0; q < 4; q++) {
+                if (r0 + q < rounds) {
+                    const uint32_t rank = atomicAdd(&s_hist[key[q]], 1u);
+                    s_kr[(r0 + q) * blockDim.x + tid] = (key[q] << 16) | rank;
+                }
             }
         }
         __syncthreads();
@@ -480,12 +493,13 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ WfParams 
             s_hist[2 * tid + 1] = excl + a;
         }
         __syncthreads();
-#pragma unroll
-        for (int r = 0; r < kMaxShadeRounds; r++)
-            if (r < P.sort_material) s_perm[s_hist[key[r]] + rank[r]] = i0 + uint32_t(r) * blockDim.x + tid;
+        for (uint32_t r = 0; r < rounds; r++) {
+            const uint32_t slot = r * blockDim.x + tid, kr = s_kr[slot];
+            s_perm[s_hist[kr >> 16] + (kr & 0xffffu)] = i0 + slot;
+        }
         __syncthreads();
-        for (int r = 0; r < P.sort_material; r++) {
-            const uint32_t j = s_perm[uint32_t(r) * blockDim.x + tid];
+        for (uint32_t r = 0; r < rounds; r++) {
+            const uint32_t j = s_perm[r * blockDim.x + tid];
             shade_path(P, c, p, j, j < n);
         }
         __syncthreads();
