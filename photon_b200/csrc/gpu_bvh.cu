@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(kThreads) k_split(BuildArgs A) {
     __shared__ int s_decision[4];  // axis, plane, mid, leaf
     __shared__ float s_geom[6];    // lo[3], scale[3]
     __shared__ int s_usable[3];
-    __shared__ int s_true, s_lcount;
+    __shared__ int s_true;
     const Task t = A.tasks[blockIdx.x];
     const int tid = threadIdx.x, B = A.bins;
     if (tid < 12) s_box[tid] = (tid % 6) < 3 ? kBig : -kBig;
