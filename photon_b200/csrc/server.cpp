@@ -409,6 +409,7 @@ void Server::loop() {
     double busy_since = -1;
     int cur = 0;
     while (!stop_) {
+        std::vector<Request*> released;  // a read-back batch's snapshot, dropped under the lock
         try {
             // Admission in arrival order while the budget allows, then chunks of work.
             while (!queue_.empty()) {
@@ -494,7 +495,7 @@ void Server::loop() {
                 PTW_CUDA(cudaEventRecord(B.ev, stream_));
                 B.in_flight = true;
             }
-            std::vector<Request*> finished, cancelled, released;
+            std::vector<Request*> finished, cancelled;
             if (P.in_flight) {
                 PTW_CUDA(cudaEventSynchronize(P.ev));
                 P.in_flight = false;
@@ -577,9 +578,11 @@ void Server::loop() {
             }
             if (!done.empty() || !cancelled.empty()) cv_done_.notify_all();
             release_batch_refs(released);
+            released.clear();
             cur ^= 1;
         } catch (const Error& e) {
             if (!lk.owns_lock()) lk.lock();
+            release_batch_refs(released);
             cudaStreamSynchronize(stream_);
             cudaStreamSynchronize(fin_stream_);
             cudaGetLastError();
