@@ -235,7 +235,8 @@ typedef struct pt_tuning {
     int32_t trace_block;       /* threads per block of the traversal kernels */
     int32_t shade_block;       /* threads per block of the shading kernel */
     int32_t sort_by_material;  /* k in 1-4: the shading kernel groups windows of k x shade_block paths by material
-                                  class before shading them; 0: queue order; -1 keep */
+                                  class before shading them (4k x shade_block on iterations whose rays
+                                  are sorted afterwards); 0: queue order; -1 keep */
     int32_t graph_bounces;     /* bounce iterations captured per CUDA graph launch */
     int32_t sort_rays;         /* 0 off, 1-6: sort continuing rays by direction octant + Morton origin cell
                                   with this many bits per axis before tracing them, on iterations of at
