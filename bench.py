@@ -11,8 +11,13 @@ scaling, replicas: no collective on the data path).
 
 Also reported: `e2e` (pt_render + pt_download_image into a host buffer, wall clock per step), the
 roofline of the dominant kernel from the library's per-kernel event timing and traversal counters,
-clocks sampled with nvidia-smi during the timed region, and the reference CPU renderer timed on the
-host cores on a bounded sample. `--impl reference` times only the reference CPU path.
+clocks sampled with nvidia-smi during the timed region, Photon's megakernel on the same GPU, scene and
+frame (`megakernel`), and the reference CPU renderer timed on the host cores on a bounded sample.
+
+`--impl reference` times only Photon's own CPU renderer, through Photon's code alone: the scene is the
+generator's raw meshes built by Photon's Scene::build (oracle/_ref, which carries its own copy of the
+generator), so that arm loads nothing of this library and walks Photon's tree, while this arm walks
+the tree of the library's own builder (the same meshes; different trees, same workload).
 """
 import argparse
 import json
@@ -34,10 +39,14 @@ WORKLOAD = "262,144-triangle terrain scene (value-noise height field + 200 insta
            "64 emitters, 4 punctual lights, 1024x512 HDR sky), 1920x1080, 16 spp, max depth 12, seed 1"
 # Algorithmic bytes of the traversal kernels: one 64-byte node per visit, one 48-byte triangle per test.
 NODE_BYTES, TRI_BYTES = 64, 48
-# DRAM bytes (read + write) of all k_trace launches of one frame of this workload, from one ncu capture
-# (profiles/launches_terrain262k_1080p_16spp.md): mostly the path state streaming in and the hits out;
-# the nodes and triangles stay in L2.
-TRACE_DRAM_BYTES_PER_FRAME = 2.744e9
+# DRAM bytes (read + write) per traced ray of k_trace, from an ncu capture of the 960x540x4 profile
+# case of the same scene (photon_b200/profile_case.py), scaled by the rays of a frame: mostly the path
+# state streaming in and the hits out; the nodes and triangles stay in L2.
+TRACE_DRAM_BYTES_PER_RAY = 2.744e9 / 55.2e6
+# Workload description shared by both arms (the reference arm renders a bounded sample of it).
+CONFIG = {"workload": WORKLOAD, "scene_triangles": TRIS, "width": WIDTH, "height": HEIGHT, "spp": SPP, "max_depth": DEPTH,
+          "samples_per_step": WIDTH * HEIGHT * SPP,
+          "l2": "GPU arm: 256 MiB device write between steps, outside the event pair (the CPU arm has no device L2)"}
 
 
 def dist_info():
@@ -165,22 +174,24 @@ def cpu_baseline(desc, cam, seconds_hint=20.0):
 
 
 def run_reference(args, world, rank):
-    """The reference arm: Photon's own CPU renderer on the host cores (rank 0 only)."""
+    """The reference arm: Photon's own CPU renderer (CpuRenderer::render, cpu_renderer.cpp:20-39) on all
+    host cores, rank 0 only, through Photon's code alone. The scene is the generator's raw meshes built
+    by Photon's Scene::build (scene.cpp:212-255, bvh.cpp:152-258) and the camera Photon's Camera::view of
+    the generator's camera; each step renders 1 spp of the full 1920x1080 frame, reported as a rate as
+    `photon bench` does (render_cli.cpp:319-327)."""
     if rank != 0:
         return 0
     from oracle import oracle as O
-    from photon_b200 import abi, native
+    from photon_b200 import abi  # ctypes structures only: loads no library
     if not O.reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "Photon's CPU build (oracle/_ref/libphoton_ref.so) is missing"}))
         return 0
-    g = native.terrain_scene(TRIS, SEED)
-    b = g.build()
-    cam = g.camera(WIDTH / HEIGHT)
-    ref = O.RefScene.from_desc(b.desc)
     cores = os.cpu_count() or 1
-    # Each step: 1 spp over a 960x540 window of the frame's camera (a bounded sample of the workload).
-    w, h = 960, 540
-    rs = abi.render_settings(w, h, max_depth=DEPTH, seed=SEED)
+    t0 = time.perf_counter()
+    ref = O.RefScene.generated(abi.PT_GEN_TERRAIN, TRIS, SEED, threads=cores)
+    build_s = time.perf_counter() - t0
+    cam = ref.camera(WIDTH / HEIGHT)
+    rs = abi.render_settings(WIDTH, HEIGHT, max_depth=DEPTH, seed=SEED)
     for _ in range(args.warmup):
         ref.render(cam, rs, 1, threads=cores)
     t = []
@@ -188,16 +199,57 @@ def run_reference(args, world, rank):
         _, secs = ref.render(cam, rs, 1, threads=cores)
         t.append(secs)
     total = sum(t)
-    value = args.steps * w * h / total / 1e6
-    sample = f"1 spp of a 960x540 image of the same scene and camera per step ({w * h} paths), all {cores} host threads"
+    value = args.steps * WIDTH * HEIGHT / total / 1e6
+    sample = f"1 spp of the 1920x1080 frame per step ({WIDTH * HEIGHT} paths), all {cores} host threads"
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural scene, seeded)",
-            "config": {"workload": WORKLOAD, "parallelism": "host threads"},
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural scene, seeded)", "config": dict(CONFIG),
+            "parallelism": f"{cores} host threads",
+            "scene_build": {"builder": "Photon's Scene::build of the generator's raw meshes", "seconds": build_s,
+                            "nodes": ref.desc.num_nodes, "triangles": ref.desc.num_tris},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+def megakernel(desc, cam, steps):
+    """Photon's megakernel (gpu_renderer.cu's render_kernel, built for sm_100a with Photon's flags into
+    oracle/_ref/libphoton_ref_gpu.so) on the same GPU, scene and frame, the way `photon bench` runs it
+    (render_cli.cpp:329-341): a 4-spp warm-up, then the frame's 16 spp as 8-spp launches. Device time
+    is GpuRenderer::last_frame_ms (CUDA events around each launch); wall time is also given."""
+    import ctypes as C
+    from oracle import oracle as O
+    from photon_b200 import abi
+    if not os.path.exists(O.REF_GPU_SO):
+        return {"unavailable": "Photon's CUDA build (oracle/_ref/libphoton_ref_gpu.so) is missing"}
+    L = O.reference_gpu()
+    if not L.refgpu_available():
+        return {"unavailable": "Photon's cuda_available() is false"}
+    ref_scene = O.RefScene.from_desc(desc, lib=L)
+    rs = abi.render_settings(WIDTH, HEIGHT, max_depth=DEPTH, seed=SEED)
+    g = L.refgpu_create()
+    try:
+        if not L.refgpu_upload(g, ref_scene.h):
+            return {"unavailable": "GpuRenderer::upload failed"}
+        L.refgpu_resize(g, WIDTH, HEIGHT)
+        L.refgpu_render(g, C.byref(cam), C.byref(rs), 4)
+        dev_ms, wall = 0.0, 0.0
+        for _ in range(steps):
+            L.refgpu_reset(g)
+            t0 = time.perf_counter()
+            for done in range(0, SPP, 8):
+                dev_ms += L.refgpu_render(g, C.byref(cam), C.byref(rs), min(8, SPP - done))
+            wall += time.perf_counter() - t0
+    finally:
+        L.refgpu_destroy(g)
+    samples = steps * WIDTH * HEIGHT * SPP
+    return {"msamples_per_s": samples / (dev_ms / 1000.0) / 1e6, "wall_msamples_per_s": samples / wall / 1e6,
+            "ms_per_frame": dev_ms / steps, "frames": steps,
+            "method": "GpuRenderer on the same resident scene: 4-spp warm-up, then 8-spp launches (photon bench)"}
+
+
+SERVED_RATE, SERVED_REQUESTS = 500.0, 1000
 
 
 def systems_sections(r, g, desc, rank):
@@ -205,10 +257,12 @@ def systems_sections(r, g, desc, rank):
     - batched: 64 seeded views (320x180..1920x1080, spp {1,4,16,64}, cameras on a sphere of radius
       1.5x the scene extent) in one pt_render_views call, against the same views rendered one
       pt_render call at a time;
-    - served: a Poisson stream of 400 requests at 40 req/s over the 36-triangle box and the 262K scene
-      (resolution / spp / depth drawn as in the serving configuration) through the server, against
-      the same stream rendered one request at a time in arrival order; p50/p99 latency from
-      submission to result;
+    - served: the serving configuration's Poisson stream (seed 7) over four resident scenes of 36,
+      262,144, 1,048,576 and 4,194,304 triangles under a 150 GB budget, resolution / spp / depth drawn
+      as the configuration says, at a saturating 500 req/s (1,000 requests: the offered work exceeds
+      what the GPU renders, so the throughput is the server's, not the offered load), through the
+      server against the same stream rendered one request at a time in arrival order; p50/p99 latency
+      from submission to result;
     - sessions: eight real-time SVGF sessions (1600x900, 1 spp per frame, 120-frame orbits) on host
       threads; p50/p99 frame time."""
     from photon_b200 import abi, native, serving, workloads
@@ -227,25 +281,40 @@ def systems_sections(r, g, desc, rank):
     tp = time.perf_counter() - t0
     out["batched"] = {"workload": "64 views of the 262K scene (seed 2)", "samples": total, "msamples_per_s": total / tb / 1e6,
                       "plain_msamples_per_s": total / tp / 1e6, "batched_over_plain": tp / tb, "api": "pt_render_views"}
-    gb = native.box_scene()
-    bb = gb.build()
-    server = native.Server(budget_bytes=150 << 30)
-    sid_b = server.add_scene(bb.desc)
-    sid_t = server.add_scene(desc)
-    stream = workloads.request_stream([(sid_b, bb.desc), (sid_t, desc)], 400, 40.0, seed=7)
+    # The four resident scenes of the serving configuration (the larger two built on the device).
+    scenes = [(native.box_scene(), None), (g, None), (native.terrain_scene(1 << 20, SEED), None), (native.terrain_scene(1 << 22, SEED), None)]
+    built = []
+    for k, (gs, _) in enumerate(scenes):
+        built.append(gs.build(gpu=k >= 2) if k != 1 else None)
+    descs = [built[0].desc, desc, built[2].desc, built[3].desc]
+    budget = 150 << 30
+    server = native.Server(budget_bytes=budget)
+    sids = [server.add_scene(d) for d in descs]
+    pairs = list(zip(sids, descs))
+    stream = workloads.request_stream(pairs, SERVED_REQUESTS, SERVED_RATE, seed=7)
     # Warm-up for both forms: a burst of 64 requests of another stream (first-time memory pinning
     # and pool growth stay out of the measurement).
-    warm = [dict(x, t=0.0) for x in workloads.request_stream([(sid_b, bb.desc), (sid_t, desc)], 64, 40.0, seed=8)]
+    warm = [dict(x, t=0.0) for x in workloads.request_stream(pairs, 64, SERVED_RATE, seed=8)]
     serving.run_served(server, warm)
     served = serving.run_served(server, stream)
     server.close()
-    rb = native.Renderer(r_device(r))
-    rb.upload(bb.desc)
-    serving.run_plain({sid_b: rb, sid_t: r}, warm)
-    plain = serving.run_plain({sid_b: rb, sid_t: r}, stream)
-    rb.close()
-    out["served"] = {"workload": "Poisson, 400 requests at 40 req/s, seed 7, scenes: 36-triangle box + 262K terrain",
-                     "served": served, "plain": plain, "budget_bytes": 150 << 30}
+    plain_r = {}
+    for sid, d in pairs:
+        if d is desc:
+            plain_r[sid] = r
+        else:
+            rr = native.Renderer(r_device(r))
+            rr.upload(d)
+            plain_r[sid] = rr
+    serving.run_plain(plain_r, warm)
+    plain = serving.run_plain(plain_r, stream)
+    for rr in plain_r.values():
+        if rr is not r:
+            rr.close()
+    out["served"] = {"workload": f"Poisson, {SERVED_REQUESTS} requests at {SERVED_RATE:g} req/s (saturating), seed 7, "
+                                 "scenes of 36 / 262,144 / 1,048,576 / 4,194,304 triangles, 150 GB budget",
+                     "served": served, "plain": plain, "budget_bytes": budget,
+                     "served_over_plain": served["msamples_per_s"] / plain["msamples_per_s"]}
     from photon_b200 import sessions
     out["sessions"] = dict(sessions.run_sessions(desc, 8, 120, 1600, 900),
                            workload="8 real-time SVGF sessions, 120-frame orbits (0.5 deg/frame) of the 262K scene, 1600x900, 1 spp",
@@ -350,30 +419,40 @@ def main():
     peak, peak_kind = measured_peak()
     trace_launches = max(1, prof.trace.launches)
     achieved = (trace_bytes_per_frame * args.steps) / (prof.trace.ms / 1000.0) / 1e9 if prof.trace.ms > 0 else 0.0
-    roofline = {"bound": "hbm", "kernel": "k_trace (closest-hit BVH traversal)", "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
-                "traffic": TRACE_DRAM_BYTES_PER_FRAME * args.steps / trace_launches,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one frame's k_trace launches",
+    shadow_achieved = (shadow_bytes_per_frame * args.steps) / (prof.shadow.ms / 1000.0) / 1e9 if prof.shadow.ms > 0 else 0.0
+    # The scene (nodes, triangles) stays in the 126 MB L2 during a frame, so the walk's bytes are L2
+    # (and L1) traffic: the live L2 read probe is the bandwidth they are bounded by. The HBM fraction
+    # is kept beside it because the copy bandwidth is the measured peak of the schema.
+    l2_peak = native.l2_read_bandwidth(local)
+    closest_rays_frame = counts.closest_rays  # the counted render is one frame
+    roofline = {"bound": "hbm", "limiter": "L2/L1 latency and issue: the scene is L2-resident (see l2, simt)",
+                "kernel": "k_trace (closest-hit BVH traversal)",
+                "l2": {"achieved": achieved, "peak": l2_peak, "unit": "GB/s", "frac": achieved / l2_peak if l2_peak > 0 else None,
+                       "peak_source": "live pt_measure_l2_bandwidth: 32 MiB L2-resident buffer read 64 times per launch "
+                                      "(ld.global.cg), best of 5"},
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+                "traffic": TRACE_DRAM_BYTES_PER_RAY * closest_rays_frame * args.steps / trace_launches,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per traced ray of k_trace on the "
+                                  "960x540x4 profile case, times this frame's rays per launch",
                 "algorithmic_bytes_per_launch": trace_bytes_per_frame * args.steps / trace_launches,
                 "avg_launch_ms": prof.trace.ms / trace_launches,
                 "model": "64 B per node visit + 48 B per triangle test (closest-hit rays)",
                 "node_visits_per_ray": counts.closest_node_visits / max(1, counts.closest_rays),
                 "tri_tests_per_ray": counts.closest_tri_tests / max(1, counts.closest_rays),
-                "shadow_bytes_per_frame": shadow_bytes_per_frame}
-    # The scene stays in L2, so the same bytes are also read against a live L2 read probe.
-    l2_peak = native.l2_read_bandwidth(local)
-    roofline["l2"] = {"peak": l2_peak, "unit": "GB/s", "frac": achieved / l2_peak if l2_peak > 0 else None,
-                      "peak_source": "live pt_measure_l2_bandwidth: 32 MiB L2-resident buffer read 64 times per "
-                                     "launch (ld.global.cg), best of 5"}
+                # Live SIMT use of the two walks from the counted render: live lanes per walk step, of 32.
+                "simt": {"trace_lanes_per_step": counts.closest_lane_steps / max(1, counts.closest_warp_steps),
+                         "shadow_lanes_per_step": counts.shadow_lane_steps / max(1, counts.shadow_warp_steps),
+                         "of": 32},
+                "shadow": {"kernel": "k_shadow (any-hit BVH traversal)", "bytes_per_frame": shadow_bytes_per_frame,
+                           "ms_per_frame": prof.shadow.ms / args.steps, "achieved": shadow_achieved,
+                           "l2_frac": shadow_achieved / l2_peak if l2_peak > 0 else None, "hbm_frac": shadow_achieved / peak}}
     rays_per_sample = (counts.closest_rays + counts.shadow_rays) / samples_per_step
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (procedural scene, seeded; no dataset)",
-            "config": {"workload": WORKLOAD, "scene_triangles": desc.num_tris, "width": WIDTH, "height": HEIGHT,
-                       "spp": SPP, "max_depth": DEPTH, "samples_per_step": samples_per_step,
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "l2": "flushed between steps (256 MiB write, outside the event pair)"},
+            "config": dict(CONFIG), "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 64 + 36 + 256,
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 12, "api": "pt_reset + pt_render + pt_download_image"},
             "gpu_launches": prof.kernel_launches,
@@ -383,6 +462,12 @@ def main():
             "kernel_share": {k: v / ktotal for k, v in kernels.items()},
             "roofline": roofline,
             "clocks": clock_info}
+    if rank == 0 and world == 1:
+        mk = megakernel(desc, cam, 3)
+        if "msamples_per_s" in mk:
+            mk["wavefront_over_megakernel"] = value / mk["msamples_per_s"]
+            mk["wavefront_e2e_over_megakernel"] = e2e_value / mk["msamples_per_s"]
+        line["megakernel"] = mk
     if not args.no_systems:
         line.update(systems_sections(r, g, desc, rank))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

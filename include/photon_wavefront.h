@@ -248,6 +248,10 @@ typedef struct pt_tuning {
                                   runs on the device, 65,536 otherwise and in the server */
     int32_t wide_shadows;      /* 1: shadow rays walk a 4-wide BVH collapsed from the scene's BVH2 (same
                                   answers), 0 (default): the BVH2; -1 keep */
+    int32_t trace_refill;      /* 1-32: a warp of the closest-hit walk claims new rays for its idle lanes
+                                  once fewer than this many lanes hold a ray (1: only when all have
+                                  finished, 32 rays at a time); <= 0 keep */
+    int32_t shadow_refill;     /* the same for the shadow (any-hit) walk; <= 0 keep */
 } pt_tuning;
 int32_t pt_set_tuning(pt_renderer* r, const pt_tuning* t);
 int32_t pt_get_tuning(const pt_renderer* r, pt_tuning* t);
@@ -277,6 +281,10 @@ typedef struct pt_profile {
     uint64_t closest_rays, shadow_rays;             /* rays traced (camera + extension, shadow) */
     uint64_t closest_node_visits, closest_tri_tests;/* with PT_PROFILE_TRAVERSAL_COUNTS */
     uint64_t shadow_node_visits, shadow_tri_tests;
+    /* SIMT use of the trace and shadow walks (with PT_PROFILE_TRAVERSAL_COUNTS): lane steps (a node
+     * visit or triangle test of one ray) and warp steps (walk-loop iterations of a warp with a live
+     * lane); lane_steps / warp_steps = live lanes per step, out of 32. The tail kernel is not counted. */
+    uint64_t closest_lane_steps, closest_warp_steps, shadow_lane_steps, shadow_warp_steps;
 } pt_profile;
 /* flags: PT_PROFILE_KERNEL_TIMES records CUDA events between the kernels of every bounce iteration
  * (inside the captured graphs) and sums each kernel's device time; PT_PROFILE_TRAVERSAL_COUNTS
@@ -345,7 +353,8 @@ const char* pt_svgf_last_error(const pt_svgf* s);
  * static device array of 40 MiB (524,288 pixels x 5 float4) that every GPU loading the library keeps
  * until the process exits; frames above 524,288 pixels are rejected with PT_ERR_INVALID. The first
  * call on a device looks up that array's device address (cudaGetSymbolAddress), so make it before any
- * stream capture. The call only enqueues work on `stream` (a cudaStream_t, 0 = legacy default stream)
+ * stream capture; the address is kept for the life of the process, so a device reset
+ * (cudaDeviceReset) after that first call is not supported. The call only enqueues work on `stream` (a cudaStream_t, 0 = legacy default stream)
  * and allocates nothing; every call shares the one array, so calls whose work overlaps on the GPU
  * (other streams, other threads) race — order them on one stream. */
 int32_t pt_svgf_run_noalloc(int32_t device, int32_t width, int32_t height, const float* color, const float* albedo,
@@ -430,6 +439,11 @@ int32_t pt_server_get_stats(pt_server* s, pt_server_stats* out);
 /* Test hook (host-side fault injection): the next `count` device allocations of request buffers
  * fail, so the affected requests end in PT_REQ_FAILED without touching the GPU. */
 int32_t pt_server_debug_fail_allocations(pt_server* s, int32_t count);
+/* Test hook (host-side fault injection): the next `count` finishing steps (a finished request's
+ * image being summed and queued for its copy to host memory) raise an error as a failing CUDA call
+ * would; the server fails the requests in flight, settles each one's device-memory accounting
+ * exactly once and goes on serving. */
+int32_t pt_server_debug_fail_finishing(pt_server* s, int32_t count);
 
 /* ---- scene construction (host) ----------------------------------------------------------------
  * Photon builds scenes on the host (Scene::build, scene.cpp:212-255). The library carries its own

@@ -95,6 +95,11 @@ def _bind_ref(L):
     L.ref_scene_from_raw.restype = C.c_void_p
     L.ref_scene_from_desc.argtypes = [P(abi.SceneDesc)]
     L.ref_scene_from_desc.restype = C.c_void_p
+    L.ref_generated_scene.argtypes = [C.c_int, C.c_int64, C.c_uint64, C.c_int]
+    L.ref_generated_scene.restype = C.c_void_p
+    L.ref_generated_raw.argtypes = [C.c_int, C.c_int64, C.c_uint64, P(P(abi.RawScene))]
+    L.ref_generated_raw.restype = C.c_void_p
+    L.ref_generated_raw_free.argtypes = [C.c_void_p]
     L.ref_scene_free.argtypes = [C.c_void_p]
     L.ref_scene_desc.argtypes = [C.c_void_p]
     L.ref_scene_desc.restype = P(abi.SceneDesc)
@@ -176,6 +181,13 @@ class RefScene:
         lib = lib or reference()
         return cls(lib.ref_scene_from_desc(C.byref(desc)), lib)
 
+    @classmethod
+    def generated(cls, kind, triangles, seed, lib=None, threads=0):
+        """A benchmark scene (abi.PT_GEN_*): the seeded generator's raw meshes built by Photon's own
+        Scene::build; its camera() is Photon's Camera::view of the generator's look-at camera."""
+        lib = lib or reference()
+        return cls(lib.ref_generated_scene(kind, triangles, seed, threads), lib)
+
     @property
     def desc(self):
         return self.lib.ref_scene_desc(self.h).contents
@@ -219,6 +231,26 @@ class RefScene:
         try:
             if self.h:
                 self.lib.ref_scene_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class RefGeneratedRaw:
+    """The generator's raw arrays as the reference library's copy of the generator makes them."""
+
+    def __init__(self, kind, triangles, seed, lib=None):
+        self.lib = lib or reference()
+        p = P(abi.RawScene)()
+        self.h = self.lib.ref_generated_raw(kind, triangles, seed, C.byref(p))
+        if not self.h:
+            raise RuntimeError("generator rejected the arguments")
+        self.raw = p.contents
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.lib.ref_generated_raw_free(self.h)
                 self.h = None
         except Exception:
             pass

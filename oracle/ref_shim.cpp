@@ -5,6 +5,9 @@
 // between the C-ABI types of include/photon_wavefront.h and Photon's C++ types, then calls Photon:
 //   - Scene::build (src/scene/scene.cpp:212-255) on raw meshes, or make_builtin_scene
 //     (src/scene/builtin.cpp:102-186);
+//   - the benchmark's procedural scenes: the raw meshes of this repository's seeded generator
+//     (photon_b200/csrc/scene_gen.cpp, compiled in by oracle/Makefile: it is the workload's
+//     definition, not the renderer) handed to Photon's Scene::build, with Photon's Camera::view;
 //   - CpuRenderer::render (src/render/cpu_renderer.cpp:20-39) for images;
 //   - render_sample's first steps (src/render/pixel.h:18-24), intersect (src/render/traverse.h:140),
 //     surface_at / Bsdf / sample_alias / find_interval (integrator.h, bsdf.h, lights.h) for the
@@ -25,6 +28,8 @@
 #include "scene/scene.h"
 
 #include "photon_wavefront.h"
+#include "pt_error.h"
+#include "scene_build.h"
 
 using namespace photon;
 
@@ -209,10 +214,13 @@ void* ref_builtin_scene(const char* name, int flat_normals) {
     return r.release();
 }
 
-// A raw scene built by Photon's Scene::build (its BVH builder and light tables).
-void* ref_scene_from_raw(const pt_raw_scene* w, int bins, int max_leaf, int threads) {
-    auto r = std::make_unique<RefScene>();
-    Scene& s = r->scene;
+}  // extern "C"
+
+namespace {
+
+// Photon's Scene from raw meshes, built by Scene::build (its BVH builder and light tables).
+void build_from_raw(RefScene& r, const pt_raw_scene* w, int bins, int max_leaf, int threads) {
+    Scene& s = r.scene;
     s.positions = copy_array<vec3>(w->positions, size_t(w->num_positions));
     if (w->normals) s.normals = copy_array<vec3>(w->normals, size_t(w->num_positions));
     if (w->uvs) s.uvs = copy_array<vec2>(w->uvs, size_t(w->num_positions));
@@ -242,10 +250,58 @@ void* ref_scene_from_raw(const pt_raw_scene* w, int bins, int max_leaf, int thre
     if (max_leaf > 0) opt.max_leaf_size = max_leaf;
     opt.threads = threads;
     s.build(opt);
-    fill_desc(*r);
-    fill_raw(*r);
+    fill_desc(r);
+    fill_raw(r);
+}
+
+}  // namespace
+
+extern "C" {
+
+// A raw scene built by Photon's Scene::build (its BVH builder and light tables).
+void* ref_scene_from_raw(const pt_raw_scene* w, int bins, int max_leaf, int threads) {
+    auto r = std::make_unique<RefScene>();
+    build_from_raw(*r, w, bins, max_leaf, threads);
     return r.release();
 }
+
+// A procedural scene of the benchmark workloads (kind PT_GEN_BOX or PT_GEN_TERRAIN, triangle count,
+// seed): the generator's raw meshes, built by Photon's Scene::build with `threads` builder threads
+// (0: all). The scene's camera is the generator's look-at camera, so ref_scene_camera gives Photon's
+// Camera::view of it. Returns NULL if the generator rejects the arguments.
+void* ref_generated_scene(int kind, int64_t triangles, uint64_t seed, int threads) {
+    ptw::GeneratedScene g;
+    try {
+        ptw::generate_scene(kind, triangles, seed, g);
+    } catch (const ptw::Error&) {
+        return nullptr;
+    }
+    auto r = std::make_unique<RefScene>();
+    build_from_raw(*r, &g.raw, 0, 0, threads);
+    Camera& c = r->scene.camera;
+    c.position = vec3(g.cam_pos.x, g.cam_pos.y, g.cam_pos.z);
+    c.target = vec3(g.cam_target.x, g.cam_target.y, g.cam_target.z);
+    c.up = vec3(g.cam_up.x, g.cam_up.y, g.cam_up.z);
+    c.vfov = g.vfov_deg;
+    c.aperture = 0.0f;
+    c.focus_distance = 0.0f;
+    return r.release();
+}
+
+// The generator's raw arrays alone (no build), for checking that this library's copy of the
+// generator produces what the product library's pt_generate_scene produces. Free with
+// ref_generated_raw_free.
+void* ref_generated_raw(int kind, int64_t triangles, uint64_t seed, const pt_raw_scene** raw) {
+    auto g = std::make_unique<ptw::GeneratedScene>();
+    try {
+        ptw::generate_scene(kind, triangles, seed, *g);
+    } catch (const ptw::Error&) {
+        return nullptr;
+    }
+    *raw = &g->raw;
+    return g.release();
+}
+void ref_generated_raw_free(void* g) { delete static_cast<ptw::GeneratedScene*>(g); }
 
 // A scene whose built arrays are copied from a description (any builder).
 void* ref_scene_from_desc(const pt_scene_desc* d) {

@@ -158,7 +158,8 @@ class Stats(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("path_capacity", C.c_int32), ("trace_block", C.c_int32), ("shade_block", C.c_int32),
                 ("sort_by_material", C.c_int32), ("graph_bounces", C.c_int32), ("sort_rays", C.c_int32),
-                ("packed", C.c_int32), ("tail_paths", C.c_int32), ("wide_shadows", C.c_int32)]
+                ("packed", C.c_int32), ("tail_paths", C.c_int32), ("wide_shadows", C.c_int32),
+                ("trace_refill", C.c_int32), ("shadow_refill", C.c_int32)]
 
 
 class KernelTime(C.Structure):
@@ -169,7 +170,9 @@ class Profile(C.Structure):
     _fields_ = [("setup", KernelTime), ("generate", KernelTime), ("trace", KernelTime), ("shade", KernelTime),
                 ("shadow", KernelTime), ("accumulate", KernelTime), ("kernel_launches", C.c_uint64),
                 ("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("closest_node_visits", C.c_uint64),
-                ("closest_tri_tests", C.c_uint64), ("shadow_node_visits", C.c_uint64), ("shadow_tri_tests", C.c_uint64)]
+                ("closest_tri_tests", C.c_uint64), ("shadow_node_visits", C.c_uint64), ("shadow_tri_tests", C.c_uint64),
+                ("closest_lane_steps", C.c_uint64), ("closest_warp_steps", C.c_uint64), ("shadow_lane_steps", C.c_uint64),
+                ("shadow_warp_steps", C.c_uint64)]
 
 
 PT_PROFILE_KERNEL_TIMES, PT_PROFILE_TRAVERSAL_COUNTS = 1, 2

@@ -363,6 +363,11 @@ int32_t pt_server_debug_fail_allocations(pt_server* s, int32_t count) {
     return guarded(&server_error, [&] { s->s->inject_allocation_failures(count); });
 }
 
+int32_t pt_server_debug_fail_finishing(pt_server* s, int32_t count) {
+    if (!s || count < 0) return PT_ERR_INVALID;
+    return guarded(&server_error, [&] { s->s->inject_finishing_failures(count); });
+}
+
 // ---- scene construction --------------------------------------------------------------------------------
 
 int32_t pt_scene_build(const pt_raw_scene* raw, const pt_bvh_build_options* opt, pt_built_scene** out) {

@@ -8,15 +8,10 @@
 #include <vector>
 
 #include "photon_wavefront.h"
+#include "pt_error.h"
 #include "pt_types.h"
 
 namespace ptw {
-
-// Thrown inside the library and turned into status codes at the C boundary.
-struct Error {
-    int32_t code;
-    std::string message;
-};
 
 #define PTW_CUDA(x)                                                                                   \
     do {                                                                                              \

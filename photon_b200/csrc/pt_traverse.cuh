@@ -23,6 +23,7 @@ struct Hit {
 
 struct TraversalCounters {
     uint32_t nodes, tris;
+    uint32_t steps;  // walk steps of the rays (lane steps of a queue walk)
 };
 
 PT_HD float safe_inv(float x) { return fabsf(x) > 1e-20f ? 1.0f / x : copysignf(1e20f, x); }

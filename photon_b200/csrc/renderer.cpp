@@ -155,6 +155,8 @@ WfParams WavefrontEngine::params(const DevScene* scenes, int single, const DevVi
     p.sort_material = tuning_.sort_by_material;
     p.tail_paths = tuning_.tail_paths == kTailAuto ? 1u : uint32_t(std::max(0, tuning_.tail_paths));
     p.wide_shadows = tuning_.wide_shadows;
+    p.trace_refill = uint32_t(std::clamp(tuning_.trace_refill, 1, 32));
+    p.shadow_refill = uint32_t(std::clamp(tuning_.shadow_refill, 1, 32));
     p.keys = keys_.ptr;
     p.hist = hist_.ptr;
     p.offsets = offsets_.ptr;
@@ -444,6 +446,10 @@ void Renderer::render_pass_set(std::vector<DevView>& views, int /*spp_total*/, s
         profile_.closest_tri_tests += last_ctr_.tri_tests;
         profile_.shadow_node_visits += last_ctr_.shadow_node_visits;
         profile_.shadow_tri_tests += last_ctr_.shadow_tri_tests;
+        profile_.closest_lane_steps += last_ctr_.trace_lane_steps;
+        profile_.closest_warp_steps += last_ctr_.trace_warp_steps;
+        profile_.shadow_lane_steps += last_ctr_.shadow_lane_steps;
+        profile_.shadow_warp_steps += last_ctr_.shadow_warp_steps;
         bool timed = engine_->profiling() & PT_PROFILE_KERNEL_TIMES;
         cudaError_t stale = cudaGetLastError();
         if (stale != cudaSuccess) throw Error{PT_ERR_CUDA, std::string("after the wavefront pass: ") + cudaGetErrorString(stale)};
@@ -674,6 +680,9 @@ void Renderer::set_tuning(const pt_tuning& t) {
     if (t.packed >= 0) cur.packed = t.packed ? 1 : 0;
     if (t.tail_paths >= 0 || t.tail_paths == kTailAuto) cur.tail_paths = t.tail_paths;
     if (t.wide_shadows >= 0) cur.wide_shadows = t.wide_shadows ? 1 : 0;
+    if (t.trace_refill > 32 || t.shadow_refill > 32) throw Error{PT_ERR_INVALID, "trace_refill and shadow_refill must be in [1, 32]"};
+    if (t.trace_refill > 0) cur.trace_refill = t.trace_refill;
+    if (t.shadow_refill > 0) cur.shadow_refill = t.shadow_refill;
     engine_->set_tuning(cur);
 }
 
@@ -688,6 +697,8 @@ void Renderer::get_tuning(pt_tuning* t) const {
     t->packed = c.packed;
     t->tail_paths = c.tail_paths;
     t->wide_shadows = c.wide_shadows;
+    t->trace_refill = c.trace_refill;
+    t->shadow_refill = c.shadow_refill;
 }
 
 // Coordinate descent over the knobs, one at a time, each candidate timed on the same probe (a view

@@ -36,6 +36,8 @@ struct Tuning {
     int packed = 1;                // f32x2 slab tests
     int wide_shadows = 0;          // 1: shadow rays walk the 4-wide BVH (measured slower on the 262K scene)
     int tail_paths = kTailAuto;    // finish the last queued paths one thread each below this many (0: never)
+    int trace_refill = 16;         // a closest-hit warp claims new rays once fewer than this many lanes hold one
+    int shadow_refill = 16;        // the same for the shadow walk
 };
 
 // Runs wavefront passes over a table of views on one device stream. Owns the path pool, the

@@ -15,7 +15,7 @@
 #include <cmath>
 #include <cstring>
 
-#include "device_scene.h"
+#include "pt_error.h"
 #include "scene_build.h"
 
 namespace ptw {

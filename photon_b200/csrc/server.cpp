@@ -253,6 +253,8 @@ void Server::inject_allocation_failures(int n) {
     inject_failures_ = n;
 }
 
+void Server::inject_finishing_failures(int n) { inject_finish_failures_.store(n); }
+
 // Called with the lock held: drops the references of a completed batch's snapshot, erasing the
 // requests that were fetched meanwhile.
 void Server::release_batch_refs(const std::vector<Request*>& reqs) {
@@ -410,6 +412,7 @@ void Server::loop() {
     int cur = 0;
     while (!stop_) {
         std::vector<Request*> released;  // a read-back batch's snapshot, dropped under the lock
+        std::vector<Request*> done;      // requests whose image has landed in host memory this turn
         try {
             // Admission in arrival order while the budget allows, then chunks of work.
             while (!queue_.empty()) {
@@ -535,6 +538,8 @@ void Server::loop() {
                     PTW_CUDA(cudaEventCreateWithFlags(&f.ev, cudaEventDisableTiming));
                     PTW_CUDA(cudaEventRecord(f.ev, fin_stream_));
                     finishing_.push_back(f);
+                    if (inject_finish_failures_.load() > 0 && inject_finish_failures_.fetch_sub(1) > 0)
+                        throw Error{PT_ERR_CUDA, "injected failure while finishing a request"};
                 }
                 for (Request* r : cancelled) release_buffers(*r, stream_);
                 released = std::move(P.reqs);
@@ -543,7 +548,6 @@ void Server::loop() {
             // Images whose copy has landed: normalise by the sample count. With nothing else to do,
             // wait for the oldest copy instead of polling.
             if (!launch && !finishing_.empty() && finished.empty()) PTW_CUDA(cudaEventSynchronize(finishing_.front().ev));
-            std::vector<Request*> done;
             for (size_t k = 0; k < finishing_.size();) {
                 Finishing& f = finishing_[k];
                 cudaError_t q = cudaEventQuery(f.ev);
@@ -591,8 +595,20 @@ void Server::loop() {
                 release_batch_refs(b.reqs);
                 b.reqs.clear();
             }
+            // Each request is settled exactly once, whichever of the lists below hold it: a request
+            // finished in this turn sits both in finishing_ and (until the lock is taken) in active_,
+            // and one whose copy landed in this turn has already left finishing_ for `done`.
+            for (Request* r : done) {
+                if (r->state != PT_REQ_RUNNING) continue;
+                r->state = PT_REQ_DONE;  // its image is in host memory
+                r->done_s = now();
+                bytes_in_use_ -= r->bytes;
+                st_.completed++;
+                st_.samples_done += r->work;
+            }
             for (Finishing& f : finishing_) {
                 cudaEventDestroy(f.ev);
+                if (f.r->state != PT_REQ_RUNNING) continue;
                 f.r->state = PT_REQ_FAILED;
                 f.r->error = e.message;
                 f.r->done_s = now();
@@ -602,6 +618,10 @@ void Server::loop() {
             // A device failure fails every running request; the server keeps its handle valid.
             for (uint64_t id : active_) {
                 Request& r = *requests_[id];
+                if (r.state != PT_REQ_RUNNING) {  // settled above
+                    release_buffers(r, stream_);
+                    continue;
+                }
                 r.state = PT_REQ_FAILED;
                 r.error = e.message;
                 r.done_s = now();

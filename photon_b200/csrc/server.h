@@ -31,6 +31,9 @@ public:
 
     // Host-side fault injection for tests: the next `n` device allocations of request buffers fail.
     void inject_allocation_failures(int n);
+    // Host-side fault injection for tests: the next `n` finishing steps fail (an error thrown right
+    // after a finished request has been queued for its read-back, as a failing CUDA call would).
+    void inject_finishing_failures(int n);
 
 private:
     struct Request {
@@ -128,6 +131,7 @@ private:
     size_t pool_bytes_ = 0;
     bool engine_started_ = false;
     int inject_failures_ = 0;
+    std::atomic<int> inject_finish_failures_{0};  // read by the loop outside the lock
 
     pt_server_stats st_{};
     std::chrono::steady_clock::time_point t0_;

@@ -734,7 +734,9 @@ std::mutex g_noalloc_mu;
 float4* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 
 // The device address of the scratch array on the current device (host code must not use the
-// symbol's host-side name as a device pointer). Looked up once per device.
+// symbol's host-side name as a device pointer). Looked up once per device and kept for the life of
+// the process: after a cudaDeviceReset the module may load elsewhere, so a reset after the first call
+// is not supported (the header says so).
 float4* noalloc_scratch(int device) {
     std::lock_guard<std::mutex> g(g_noalloc_mu);
     if (!g_noalloc_ptr[device]) {

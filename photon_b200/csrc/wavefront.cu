@@ -175,6 +175,56 @@ __global__ void __launch_bounds__(256) k_generate(const __grid_constant__ WfPara
     }
 }
 
+// ---- the queue walk shared by trace and shadow -------------------------------------------------------
+// Persistent walk over a ray queue with warp-granular refill (dynamic ray fetch, after Aila and Laine,
+// "Understanding the Efficiency of Ray Traversal on GPUs", HPG 2009). Each lane advances its ray one
+// walk step at a time (a node visit or a triangle test). A warp that claimed 32 rays and walked them to
+// the end would idle most lanes behind its longest ray; here, whenever fewer than `refill` lanes hold
+// a live ray and the queue is not exhausted, the idle lanes claim the next rays of the queue together
+// (one atomic per warp) and start them on the spot. A ray's walk, and so its result and its counts,
+// does not depend on the lane or the moment it starts, so every `refill` gives the same results;
+// refill = 1 claims only once all lanes have finished (32 consecutive rays at a time).
+// begin(i, w) initialises walker w from queue entry i and returns its scene; end(i, w) consumes the
+// finished walk. Count: tc.steps counts lane steps and warp_steps the loop's iterations.
+template <typename W, int Overflow, bool Count, typename Begin, typename End>
+__device__ __forceinline__ void walk_queue(uint32_t n, uint32_t* claim, uint32_t refill, int* stack, int stride, TraversalCounters& tc,
+                                           uint32_t& warp_steps, Begin begin, End end) {
+    int overflow[Overflow];
+    W w;
+    const DevScene* s = nullptr;
+    uint32_t idx = 0;
+    bool live = false, drained = false;
+    const uint32_t lane = lane_id(), below = (1u << lane) - 1u;
+    for (;;) {
+        uint32_t act = __ballot_sync(kFull, live);
+        if (!drained && uint32_t(__popc(act)) < refill) {
+            const uint32_t idle = ~act, want = uint32_t(__popc(idle));
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(claim, want);
+            base = __shfl_sync(kFull, base, 0);
+            drained = base + want >= n;
+            if (!live) {
+                const uint32_t r = base + uint32_t(__popc(idle & below));
+                if (r < n) {
+                    idx = r;
+                    s = begin(r, w);
+                    live = true;
+                }
+            }
+            act = __ballot_sync(kFull, live);
+        }
+        if (act == 0) break;
+        if (Count) warp_steps++;
+        if (live) {
+            if (Count) tc.steps++;
+            if (!w.step(*s, stack, stride, overflow, &tc)) {
+                end(idx, w);
+                live = false;
+            }
+        }
+    }
+}
+
 // ---- trace: closest hit (traverse.h:140-142) -------------------------------------------------------
 template <bool Count, bool Packed>
 __global__ void __launch_bounds__(256) k_trace(const __grid_constant__ WfParams P) {
@@ -183,23 +233,25 @@ __global__ void __launch_bounds__(256) k_trace(const __grid_constant__ WfParams 
     Counters* c = P.ctr;
     if (c->tail) return;
     const uint32_t p = c->parity, n = c->count[p];
-    TraversalCounters tc{0, 0};
-    for (;;) {
-        uint32_t i0 = warp_fetch(&c->fetch[1]);
-        if (i0 >= n) break;
-        uint32_t i = i0 + lane_id();
-        if (i < n) {
-            float4 o4 = P.pb.o[p][i], d4 = P.pb.d[p][i];
-            int view = P.single_scene >= 0 ? 0 : int(P.pb.id[p][i].x);
-            const DevScene& s = scene_for(P, view);
-            Hit h{kInf, -1, 0.0f, 0.0f};
-            traverse<false, Count, Packed>(s, xyz(o4), xyz(d4), kInf, h, stack, blockDim.x, &tc);
-            P.pb.hit[i] = make_float4(h.t, __int_as_float(h.tri), h.u, h.v);
-        }
-    }
+    TraversalCounters tc{0, 0, 0};
+    uint32_t warp_steps = 0;
+    using W = Walker<false, Count, Packed>;
+    walk_queue<W, kStackSize - kSmemStack, Count>(
+        n, &c->fetch[1], P.trace_refill, stack, blockDim.x, tc, warp_steps,
+        [&](uint32_t i, W& w) -> const DevScene* {
+            const float4 o4 = P.pb.o[p][i], d4 = P.pb.d[p][i];
+            const DevScene* s = &scene_for(P, P.single_scene >= 0 ? 0 : int(P.pb.id[p][i].x));
+            w.init(xyz(o4), xyz(d4), kInf);
+            return s;
+        },
+        [&](uint32_t i, const W& w) {
+            P.pb.hit[i] = w.tri >= 0 ? make_float4(w.tmax, __int_as_float(w.tri), w.u, w.v) : make_float4(kInf, __int_as_float(-1), 0.0f, 0.0f);
+        });
     if (Count) {
         warp_add_u64(&c->node_visits, tc.nodes);
         warp_add_u64(&c->tri_tests, tc.tris);
+        warp_add_u64(&c->trace_lane_steps, tc.steps);
+        if (lane_id() == 0) atomicAdd(&c->trace_warp_steps, (unsigned long long)warp_steps);
     }
 }
 
@@ -561,6 +613,8 @@ __global__ void __launch_bounds__(256) k_tail(const __grid_constant__ WfParams P
 // ---- shadow: any hit (traverse.h:144-147) --------------------------------------------------------------
 // Capped at 51 registers (five 256-thread blocks per SM): the any-hit walk gains more from the extra
 // resident warps than it loses to the tighter allocation (measured; the closest-hit walk does not).
+// Wide: the 4-wide BVH, used when every ray of the launch has it (a single scene that carries one);
+// otherwise the BVH2.
 template <bool Count, bool Packed, bool Wide>
 __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfParams P) {
     extern __shared__ int smem_stack[];
@@ -568,38 +622,49 @@ __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfPar
     Counters* c = P.ctr;
     if (c->tail) return;
     const uint32_t q = c->parity ^ 1u, n = c->shadow_count;
-    TraversalCounters tc{0, 0};
-    for (;;) {
-        uint32_t i0 = warp_fetch(&c->fetch[3]);
-        if (i0 >= n) break;
-        uint32_t i = i0 + lane_id();
-        if (i >= n) continue;
-        float4 a = P.pb.sh0[i], b = P.pb.sh1[i], cc = P.pb.sh2[i];
-        uint32_t tag = __float_as_uint(cc.w);
-        uint32_t view = tag & 0x7fffffffu;
-        const DevScene& s = scene_for(P, int(view));
-        Hit h{kInf, -1, 0.0f, 0.0f};
-        bool occ = (Wide && s.nodes4) ? occluded4<Count, Packed>(s, xyz(a), xyz(b), a.w, stack, blockDim.x, &tc)
-                                      : traverse<true, Count, Packed>(s, xyz(a), xyz(b), a.w, h, stack, blockDim.x, &tc);
-        if (!occ) {
-            uint32_t target = __float_as_uint(b.w);
-            if (tag & 0x80000000u) {
-                float4* so = P.views[view].sample_out + target;
-                float4 l = *so;
-                *so = make_float4(l.x + cc.x, l.y + cc.y, l.z + cc.z, l.w);
-            } else {
-                float4 b4 = P.pb.beta[q][target], l4 = P.pb.lr[q][target];
-                b4.w = b4.w + cc.x;
-                l4.x = l4.x + cc.y;
-                l4.y = l4.y + cc.z;
-                P.pb.beta[q][target] = b4;
-                P.pb.lr[q][target] = l4;
-            }
+    TraversalCounters tc{0, 0, 0};
+    uint32_t warp_steps = 0;
+    auto begin = [&](uint32_t i, auto& w) -> const DevScene* {
+        const float4 a = P.pb.sh0[i], b = P.pb.sh1[i];
+        const DevScene* s = &scene_for(P, P.single_scene >= 0 ? 0 : int(__float_as_uint(P.pb.sh2[i].w) & 0x7fffffffu));
+        w.init(xyz(a), xyz(b), a.w);
+        return s;
+    };
+    // An unoccluded shadow ray adds its contribution to its path (or to its finished sample).
+    auto deliver = [&](uint32_t i) {
+        const float4 cc = P.pb.sh2[i];
+        const uint32_t tag = __float_as_uint(cc.w), view = tag & 0x7fffffffu, target = __float_as_uint(P.pb.sh1[i].w);
+        if (tag & 0x80000000u) {
+            float4* so = P.views[view].sample_out + target;
+            float4 l = *so;
+            *so = make_float4(l.x + cc.x, l.y + cc.y, l.z + cc.z, l.w);
+        } else {
+            float4 b4 = P.pb.beta[q][target], l4 = P.pb.lr[q][target];
+            b4.w = b4.w + cc.x;
+            l4.x = l4.x + cc.y;
+            l4.y = l4.y + cc.z;
+            P.pb.beta[q][target] = b4;
+            P.pb.lr[q][target] = l4;
         }
+    };
+    if (Wide && P.single_scene >= 0 && P.scenes[P.single_scene].nodes4) {
+        using W4 = AnyWalker4<Count, Packed>;
+        walk_queue<W4, kBvh4Stack - kSmemStack, Count>(n, &c->fetch[3], P.shadow_refill, stack, blockDim.x, tc, warp_steps, begin,
+                                                       [&](uint32_t i, const W4& w) {
+                                                           if (!w.hit) deliver(i);
+                                                       });
+    } else {
+        using W = Walker<true, Count, Packed>;
+        walk_queue<W, kStackSize - kSmemStack, Count>(n, &c->fetch[3], P.shadow_refill, stack, blockDim.x, tc, warp_steps, begin,
+                                                      [&](uint32_t i, const W& w) {
+                                                          if (w.tri < 0) deliver(i);
+                                                      });
     }
     if (Count) {
         warp_add_u64(&c->shadow_node_visits, tc.nodes);
         warp_add_u64(&c->shadow_tri_tests, tc.tris);
+        warp_add_u64(&c->shadow_lane_steps, tc.steps);
+        if (lane_id() == 0) atomicAdd(&c->shadow_warp_steps, (unsigned long long)warp_steps);
     }
 }
 

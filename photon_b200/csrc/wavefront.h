@@ -56,6 +56,10 @@ struct Counters {
     unsigned long long rays, shadow_rays, paths_done;
     unsigned long long node_visits, tri_tests;
     unsigned long long shadow_node_visits, shadow_tri_tests;
+    // SIMT use of the queue walks (k_trace, k_shadow), counted with the traversal counters: lane
+    // steps (one node visit or triangle test of one ray) and warp steps (iterations of a warp's walk
+    // loop with a live lane); lane steps / warp steps = live lanes per step out of 32.
+    unsigned long long trace_lane_steps, trace_warp_steps, shadow_lane_steps, shadow_warp_steps;
 };
 
 struct PathBuffers {
@@ -83,6 +87,8 @@ struct WfParams {
     uint32_t tail_paths;       // > 0: once no new paths remain and at most Counters::tail_limit are queued,
                                // finish them in one kernel (one thread per path, all bounces)
     int wide_shadows;          // 1: shadow rays walk the 4-wide BVH where the scene has one
+    uint32_t trace_refill;     // 1-32: a trace warp claims new rays once fewer of its lanes hold one
+    uint32_t shadow_refill;    // the same for the shadow walk
     int sort_material;         // 1: the shade kernel groups each block's paths by material class
     int sort_bits;             // > 0: sort continuing paths by direction octant + Morton origin cell
                                //      (this many bits per axis) before they are traced

@@ -90,6 +90,7 @@ def _load():
         "pt_server_cancel": ([C.c_void_p, C.c_uint64], C.c_int32),
         "pt_server_get_stats": ([C.c_void_p, P(abi.ServerStats)], C.c_int32),
         "pt_server_debug_fail_allocations": ([C.c_void_p, C.c_int32], C.c_int32),
+        "pt_server_debug_fail_finishing": ([C.c_void_p, C.c_int32], C.c_int32),
         "pt_scene_build": ([P(abi.RawScene), P(abi.BvhBuildOptions), P(C.c_void_p)], C.c_int32),
         "pt_scene_desc_of": ([C.c_void_p], P(abi.SceneDesc)),
         "pt_scene_free": ([C.c_void_p], None),
@@ -235,7 +236,7 @@ class Renderer:
         return p
 
     def set_tuning(self, **kw):
-        t = abi.Tuning(0, 0, 0, -1, -1, -1, -1, -1, -1)
+        t = abi.Tuning(0, 0, 0, -1, -1, -1, -1, -1, -1, 0, 0)
         for k, v in kw.items():
             setattr(t, k, v)
         _check(lib.pt_set_tuning(self.h, C.byref(t)), self._err)
@@ -387,6 +388,9 @@ class Server:
 
     def fail_allocations(self, n):
         _check(lib.pt_server_debug_fail_allocations(self.h, n), self._err)
+
+    def fail_finishing(self, n):
+        _check(lib.pt_server_debug_fail_finishing(self.h, n), self._err)
 
     def close(self):
         if getattr(self, "h", None):

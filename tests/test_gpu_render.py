@@ -69,8 +69,11 @@ def test_heatmap_matches_node_visits(renderer, name):
 
 
 @pytest.mark.parametrize("name,w,h,spp", [("cornell", 96, 54, 64), ("materials", 96, 54, 64), ("glass", 96, 54, 64),
-                                          ("box", 128, 128, 64), ("terrain", 192, 108, 16)])
+                                          ("box", 256, 256, 64), ("terrain", 192, 108, 16)])
 def test_images_agree_with_oracle(renderer, name, w, h, spp):
+    """The box case is the small configuration at its stated size: the 36-triangle closed box (grey
+    0.73, red and green walls, a (17, 12, 4) ceiling emitter), 256x256 at 64 spp, max depth 8, Russian
+    roulette from depth 3, seed 1."""
     desc, camf, keep = scenes.scene(name)
     cam = camf(w / h)
     rs = _settings(name, w, h, seed=1)
@@ -213,12 +216,18 @@ def test_gpu_matches_golden_fixtures(renderer, name):
     dict(wide_shadows=1, packed=0, tail_paths=0),
     dict(tail_paths=1 << 30),
     dict(tail_paths=1 << 12, path_capacity=1 << 14, graph_bounces=0),
+    dict(tail_paths=0, trace_refill=1, shadow_refill=1),
+    dict(tail_paths=0, trace_refill=32, shadow_refill=32),
+    dict(tail_paths=0, trace_refill=5, shadow_refill=27, path_capacity=1 << 13),
+    dict(tail_paths=0, wide_shadows=1, shadow_refill=32, trace_block=256),
 ])
 def test_tuning_variants_are_bit_identical(tuning):
     """Every autotuner knob changes how the work is scheduled, never a path's arithmetic: scalar or
     packed slab tests, material-sorted shading, ray sorting, block shapes, the path pool size, the
-    graph cadence, the one-thread-per-path tail (never, always, small) and the shadow rays' BVH (4-wide
-    or Photon's BVH2) all give the same image bit for bit (accumulation is in sample order)."""
+    graph cadence, the one-thread-per-path tail (never, always, small), the shadow rays' BVH (4-wide
+    or Photon's BVH2) and when a walk's warp refills its idle lanes (only once all have finished,
+    whenever one has, in between) all give the same image bit for bit (accumulation is in sample
+    order). The variants that switch the tail off make the queued kernels walk every ray."""
     desc, camf, keep = scenes.scene("terrain")
     w, h, spp = 160, 90, 4
     cam = camf(w / h)

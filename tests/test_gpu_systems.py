@@ -149,6 +149,46 @@ def test_server_budget_cancel_and_faults(server_scenes):
     s.close()
 
 
+def test_server_device_failure_while_finishing_settles_each_request_once(server_scenes):
+    """A failure raised while a finished request is being queued for its read-back (host-side
+    injection, as a failing CUDA call there would) fails the requests in flight. Each request's
+    device memory is given back exactly once: afterwards the server's memory in use is back to its
+    pool and scenes, its budget checks still admit work, and a new request renders."""
+    (bdesc, bcam, bkeep), _ = server_scenes
+    budget = 1 << 30
+    s = native.Server(budget_bytes=budget, path_capacity=1 << 16)
+    sid = s.add_scene(bdesc)
+    cam = bcam(1.0)
+    idle = s.stats().device_bytes_in_use
+    for _ in range(3):
+        s.fail_finishing(1)
+        ids = [s.submit(sid, cam, 32 + 8 * k, 32, 1 + k % 3) for k in range(6)]
+        states = []
+        for r in ids:
+            try:
+                s.wait(r, 60)
+            except native.PhotonError as e:
+                assert e.code == abi.PT_ERR_CUDA, e
+            states.append(s.poll(r))
+        assert abi.PT_REQ_FAILED in states
+        assert set(states) <= {abi.PT_REQ_FAILED, abi.PT_REQ_DONE}
+        for r in ids:
+            try:
+                s.fetch(r, 32 + 64, 32)
+            except native.PhotonError:
+                pass
+        st = s.stats()
+        assert st.active == 0 and st.queued == 0
+        assert st.device_bytes_in_use == idle, (st.device_bytes_in_use, idle)
+    ok = s.submit(sid, cam, 64, 64, 4)
+    s.wait(ok, 60)
+    assert s.poll(ok) == abi.PT_REQ_DONE
+    img, _ = s.fetch(ok, 64, 64)
+    assert np.isfinite(img).all() and img.mean() > 0
+    assert s.stats().device_bytes_in_use == idle
+    s.close()
+
+
 def test_server_cancels_running_and_queued_requests(server_scenes):
     """One request runs at a time (max_active 1): a long request on the 262K scene is cancelled while
     it runs and three others while they wait; all end cancelled, their buffers are released, and the

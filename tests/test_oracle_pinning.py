@@ -225,3 +225,50 @@ def test_alpha_masked_triangles_are_skipped_known_answer():
         t, tri = hits[0, 0, 0], O.hits_tri(hits)[0, 0]
         assert abs(t - 5) < 1e-4
         assert d.tris[tri].material == 1
+
+
+def _raw_arrays(raw):
+    """Every array of a pt_raw_scene as bytes, by name (for byte-for-byte comparison)."""
+    n_pos, n_idx = raw.num_positions, raw.num_indices
+    out = {}
+
+    def take(name, ptr, count, itemsize):
+        out[name] = C.string_at(ptr, count * itemsize) if ptr and count else b""
+
+    take("positions", raw.positions, n_pos, 12)
+    take("normals", raw.normals, n_pos, 12)
+    take("uvs", raw.uvs, n_pos, 8)
+    take("indices", raw.indices, n_idx, 4)
+    take("tri_material", raw.tri_material, n_idx // 3, 4)
+    take("materials", raw.materials, raw.num_materials, C.sizeof(abi.Material))
+    take("punctual", raw.punctual, raw.num_punctual, C.sizeof(abi.PunctualLight))
+    take("env", raw.env_texels, raw.env_width * raw.env_height, 12)
+    for k in range(raw.num_textures):
+        t = raw.textures[k]
+        take(f"texture{k}", t.texels, t.width * t.height, 4)
+        out[f"texture{k}_info"] = (t.width, t.height, t.repeat, t.srgb)
+    out["scalars"] = (raw.env_width, raw.env_height, raw.env_color.x, raw.env_color.y, raw.env_color.z,
+                      raw.env_intensity, raw.env_rotation)
+    return out
+
+
+@needs_ref
+@pytest.mark.parametrize("kind,tris", [(abi.PT_GEN_BOX, 36), (abi.PT_GEN_TERRAIN, 262144), (abi.PT_GEN_TERRAIN, 70000)])
+def test_reference_build_holds_the_same_scene_generator(kind, tris):
+    """The benchmark's reference arm builds its scene without the product library: Photon's build
+    carries its own copy of the seeded generator. Its raw meshes, materials, textures, lights and
+    environment equal pt_generate_scene's byte for byte; Photon's Scene::build of them gives the
+    triangle count, and its camera is Photon's Camera::view of the generator's look-at camera."""
+    ours = native.GeneratedScene(kind, tris, 1)
+    theirs = O.RefGeneratedRaw(kind, tris, 1)
+    a, b = _raw_arrays(ours.raw), _raw_arrays(theirs.raw)
+    assert a.keys() == b.keys()
+    for k in a:
+        assert a[k] == b[k], k
+    s = O.RefScene.generated(kind, tris, 1, threads=4)
+    assert s.desc.num_tris == tris
+    c0, c1 = ours.camera(16 / 9), s.camera(16 / 9)
+    for f in ("position", "forward", "right", "up"):
+        v0, v1 = getattr(c0, f), getattr(c1, f)
+        assert max(abs(v0.x - v1.x), abs(v0.y - v1.y), abs(v0.z - v1.z)) < 1e-6, f
+    assert abs(c0.tan_half_fov - c1.tan_half_fov) < 1e-6 and c0.aspect == c1.aspect

@@ -1,9 +1,10 @@
-"""The allocation-free SVGF entry point (pt_svgf_run_noalloc), through the C ABI, against the
-allocating one: the first frame of a fresh pt_svgf session denoises the same G-buffers with the same
-kernels, so the two outputs agree within the SVGF tolerance (|a - b| <= 1e-4 * max(|b|, 1e-2) per
-channel) on every pixel. Two calls in a row on different frames check that the shared static scratch
-carries nothing from one call to the next. Collected last so it also runs after every other test has
-used the device."""
+"""The allocation-free SVGF entry point (pt_svgf_run_noalloc), through the C ABI, for callers that
+cannot allocate device memory. Its output is checked against the allocating entry point (the first
+frame of a fresh pt_svgf session: the same kernels on the same G-buffers) and against the oracle's
+restatement of Photon's Svgf::run on its first frame, within the SVGF tolerance
+(|a - b| <= 1e-4 * max(|b|, 1e-2) per channel) on every pixel. Two calls in a row on different frames
+check that the shared static scratch carries nothing from one call to the next. Collected last so it
+also runs after every other test has used the device."""
 import ctypes as C
 
 import numpy as np
@@ -64,7 +65,11 @@ def test_noalloc_matches_session_first_frame(torch_cuda, iterations):
         want = _allocating(torch, dev, w, h, settings, cam)
         assert np.isfinite(got).all()
         err = np.abs(got - want) / np.maximum(np.abs(want), FLOOR)
-        assert float(err.max()) <= REL, f"max relative error {float(err.max()):.3g}"
+        assert float(err.max()) <= REL, f"max relative error {float(err.max()):.3g} against pt_svgf_run"
+        # The oracle: a fresh restatement session's first frame (no history to reproject).
+        oracle = O.OrcSvgf(w, h).run(g, cam, settings)
+        err = np.abs(got - oracle) / np.maximum(np.abs(oracle), FLOOR)
+        assert float(err.max()) <= REL, f"max relative error {float(err.max()):.3g} against the oracle"
 
 
 def test_noalloc_rejects_frames_above_the_scratch(torch_cuda):
