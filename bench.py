@@ -39,10 +39,11 @@ WORKLOAD = "262,144-triangle terrain scene (value-noise height field + 200 insta
            "64 emitters, 4 punctual lights, 1024x512 HDR sky), 1920x1080, 16 spp, max depth 12, seed 1"
 # Algorithmic bytes of the traversal kernels: one 64-byte node per visit, one 48-byte triangle per test.
 NODE_BYTES, TRI_BYTES = 64, 48
-# DRAM bytes (read + write) per traced ray of k_trace, from an ncu capture of the 960x540x4 profile
-# case of the same scene (photon_b200/profile_case.py), scaled by the rays of a frame: mostly the path
-# state streaming in and the hits out; the nodes and triangles stay in L2.
-TRACE_DRAM_BYTES_PER_RAY = 2.744e9 / 55.2e6
+# DRAM bytes (read + write) per traced ray of k_trace: the first k_trace launch of the 960x540x4 profile
+# case of the same scene (photon_b200/profile_case.py; 2,073,600 camera rays, 74.59 MB read + 11.79 MB
+# written in one ncu capture), scaled by the rays of a launch here: mostly the path state streaming in
+# and the hits out; the nodes and triangles stay in L2.
+TRACE_DRAM_BYTES_PER_RAY = (74.59e6 + 11.79e6) / 2073600
 # Workload description shared by both arms (the reference arm renders a bounded sample of it).
 CONFIG = {"workload": WORKLOAD, "scene_triangles": TRIS, "width": WIDTH, "height": HEIGHT, "spp": SPP, "max_depth": DEPTH,
           "samples_per_step": WIDTH * HEIGHT * SPP,
@@ -335,6 +336,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-systems", action="store_true", help="skip the batched-views and served-stream sections")
+    ap.add_argument("--no-megakernel", action="store_true", help="skip the megakernel comparison")
     args = ap.parse_args()
     world, rank, local = dist_info()
     if args.impl == "reference":
@@ -462,7 +464,7 @@ def main():
             "kernel_share": {k: v / ktotal for k, v in kernels.items()},
             "roofline": roofline,
             "clocks": clock_info}
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_megakernel:
         mk = megakernel(desc, cam, 3)
         if "msamples_per_s" in mk:
             mk["wavefront_over_megakernel"] = value / mk["msamples_per_s"]

@@ -213,6 +213,10 @@ int32_t pt_download_display(pt_renderer* r, uint32_t* rgba8, size_t n);
 /* The G-buffer of the first sample of the last pt_render (or of the last pt_render_denoised):
  * albedo (4 floats/pixel) and normal + depth (4 floats/pixel). Either pointer may be NULL. */
 int32_t pt_download_gbuffer(pt_renderer* r, float* albedo4, float* normal_depth4, size_t n_pixels);
+/* The accumulation as it stands (a probe, like the G-buffer): per pixel the sum of the samples'
+ * radiance (rgb) and of their squared luminance (w), the inputs of pt_display's colour and variance
+ * views (GpuRenderer keeps the same sums, gpu_renderer.cu:70-79). */
+int32_t pt_download_accumulation(pt_renderer* r, float* sums4, size_t n_pixels);
 /* GpuRenderer::display_buffer (gpu_renderer.h:65): the device address of the RGBA8 buffer. */
 uint32_t* pt_display_buffer(pt_renderer* r);
 
@@ -252,6 +256,8 @@ typedef struct pt_tuning {
                                   once fewer than this many lanes hold a ray (1: only when all have
                                   finished, 32 rays at a time); <= 0 keep */
     int32_t shadow_refill;     /* the same for the shadow (any-hit) walk; <= 0 keep */
+    int32_t walk_burst;        /* walk steps each lane takes between two refill checks of its warp (1 to 2^20);
+                                  <= 0 keep */
 } pt_tuning;
 int32_t pt_set_tuning(pt_renderer* r, const pt_tuning* t);
 int32_t pt_get_tuning(const pt_renderer* r, pt_tuning* t);
@@ -395,9 +401,12 @@ typedef struct pt_server pt_server;
 typedef struct pt_server_config {
     int32_t device;
     uint64_t budget_bytes;     /* device memory for scenes + requests + path pool */
-    int32_t path_capacity;     /* shared path pool (0: 8,388,608 paths) */
+    int32_t path_capacity;     /* shared path pool (0: 16,777,216 paths) */
     int32_t max_active;        /* requests on the device at once (0: 16; negative: unbounded, budget only) */
     double device_wait_seconds;/* bound of every device-side wait (0: 2 s) */
+    int32_t sort_rays;         /* ray sorting of iterations of at least 2,097,152 paths, bits per axis of the
+                                  origin cell (1-6); 0: the default (4, while that many paths are
+                                  pending); -1: off */
 } pt_server_config;
 typedef struct pt_request {
     int32_t scene_id;

@@ -22,6 +22,7 @@
 #include <atomic>
 #include <vector>
 
+#include "core/color.h"
 #include "render/cpu_renderer.h"
 #include "render/pixel.h"
 #include "scene/builtin.h"
@@ -486,6 +487,62 @@ void ref_heatmap(void* h, const pt_camera* cam, int w, int hgt, float* out) {
             intersect(s, ray, hit, &visits);
             out[size_t(y) * size_t(w) + size_t(x)] = float(visits);
         }
+}
+
+// display_kernel's per-pixel mapping (gpu_renderer.cu:129-175) evaluated on the host with Photon's own
+// host-compiled colour functions (color.h:8-41: tone_map, srgb_to_linear, pack_rgba8; math.h:
+// luminance, saturate, lerp) and heat_color's ramp (gpu_renderer.cu:108-115): the CPU side of the
+// display comparison, against which Photon's --use_fast_math device build and the wavefront's display
+// kernel are both measured. Arguments as refgpu_display_buffers (host arrays).
+void ref_display_cpu(int w, int h, int mode, float exposure, int tonemap, float samples, float max_depth, float heat_scale, int denoised,
+                     const float* accum4, const float* denoised4, const float* albedo4, const float* normal_depth4,
+                     const float* variance4, const float* heat, uint32_t* out) {
+    const float inv_samples = samples > 0 ? 1.0f / samples : 0.0f;
+    auto v4 = [](const float* b, size_t i) { return b ? vec4(b[4 * i], b[4 * i + 1], b[4 * i + 2], b[4 * i + 3]) : vec4(0, 0, 0, 0); };
+    auto heat_color = [](float t) {
+        t = saturate(t);
+        vec3 c0(0.05f, 0.05f, 0.35f), c1(0.0f, 0.6f, 0.4f), c2(0.95f, 0.85f, 0.1f), c3(0.85f, 0.1f, 0.05f);
+        if (t < 1.0f / 3) return lerp(c0, c1, t * 3);
+        if (t < 2.0f / 3) return lerp(c1, c2, t * 3 - 1);
+        return lerp(c2, c3, t * 3 - 2);
+    };
+    for (size_t i = 0; i < size_t(w) * size_t(h); i++) {
+        vec3 c;
+        switch (mode) {
+            default:
+            case 0:
+                c = denoised ? v4(denoised4, i).xyz() : v4(accum4, i).xyz() * inv_samples;
+                c = tone_map(c, exposure, ToneMap(tonemap));
+                break;
+            case 1: c = v4(albedo4, i).xyz(); break;
+            case 2: {
+                vec4 nd = v4(normal_depth4, i);
+                c = nd.w > 0 ? nd.xyz() * 0.5f + vec3(0.5f) : vec3(0);
+                break;
+            }
+            case 3: {
+                float d = v4(normal_depth4, i).w;
+                c = d > 0 ? vec3(1.0f - saturate(d / max_depth)) : vec3(0);
+                break;
+            }
+            case 4: {
+                float v;
+                if (denoised) {
+                    v = v4(variance4, i).w;
+                } else {
+                    vec4 a = v4(accum4, i);
+                    float mean = luminance(a.xyz()) * inv_samples;
+                    v = samples > 1 ? std::fmax(0.0f, a.w * inv_samples - mean * mean) / (samples - 1) : 0.0f;
+                }
+                float t = std::sqrt(v);
+                c = vec3(t / (1.0f + t));
+                break;
+            }
+            case 5: c = heat_color((heat ? heat[i] : 0.0f) * heat_scale); break;
+        }
+        if (mode != 0 && mode != 1) c = vec3(srgb_to_linear(c.x), srgb_to_linear(c.y), srgb_to_linear(c.z));
+        out[i] = pack_rgba8(c);
+    }
 }
 
 // Photon's build_alias_table (scene.cpp:82-111) on a weight list (for known-answer tests).

@@ -182,6 +182,10 @@ int32_t pt_download_gbuffer(pt_renderer* r, float* albedo4, float* normal_depth4
     PT_RENDERER_CALL(r, r->r->download_gbuffer(albedo4, normal_depth4, n_pixels));
 }
 
+int32_t pt_download_accumulation(pt_renderer* r, float* sums4, size_t n_pixels) {
+    PT_RENDERER_CALL(r, r->r->download_accumulation(sums4, n_pixels));
+}
+
 uint32_t* pt_display_buffer(pt_renderer* r) { return r && r->r ? r->r->display_buffer() : nullptr; }
 
 int32_t pt_get_stats(const pt_renderer* r, pt_stats* out) {

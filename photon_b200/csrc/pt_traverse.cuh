@@ -26,6 +26,15 @@ struct TraversalCounters {
     uint32_t steps;  // walk steps of the rays (lane steps of a queue walk)
 };
 
+// What a walk step reads of its scene: the node array it walks (the BVH2's, or the 4-wide BVH's), the
+// triangles, and the scene for the rare alpha test. Kept apart so that a walk loop can hold the two
+// array bases in registers instead of reloading them from the scene table at every step.
+struct WalkScene {
+    const float4* nodes;
+    const float4* tris;
+    const DevScene* scene;
+};
+
 PT_HD float safe_inv(float x) { return fabsf(x) > 1e-20f ? 1.0f / x : copysignf(1e20f, x); }
 
 // Slab test (traverse.h:40-47): entry distance or kInf.
@@ -133,10 +142,10 @@ struct Walker {
     }
 
     // Advances one unit; returns false once the ray is finished.
-    PT_HD bool step(const DevScene& s, int* stack, int stride, int* overflow, TraversalCounters* cnt) {
+    PT_HD bool step(const WalkScene& ws, int* stack, int stride, int* overflow, TraversalCounters* cnt) {
         bool decide = false;
         if (!leaf_mode) {
-            const float4* n = s.nodes + 4 * node;
+            const float4* n = ws.nodes + 4 * node;
             float4 n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2), n3 = __ldg(n + 3);
             if (Count) cnt->nodes++;
             float tl = Packed ? box_entry2(n0, n1, rp, tmax) : box_entry(n0, n1, o, inv_d, tmax);
@@ -171,12 +180,12 @@ struct Walker {
         }
         if (leaf_mode) {
             int i = ti;
-            const float4* g = s.tris + 3 * i;
+            const float4* g = ws.tris + 3 * i;
             float4 g0 = __ldg(g), g1 = __ldg(g + 1), g2 = __ldg(g + 2);
             float t, tu, tv;
             if (Count) cnt->tris++;
             if (tri_intersect(g0, g1, g2, o, d, tmax, t, tu, tv) &&
-                !((__float_as_int(g1.w) & 1) && alpha_passes(s, i, __float_as_int(g0.w), tu, tv))) {
+                !((__float_as_int(g1.w) & 1) && alpha_passes(*ws.scene, i, __float_as_int(g0.w), tu, tv))) {
                 tmax = t;
                 tri = i;
                 u = tu;
@@ -223,7 +232,8 @@ PT_HD bool traverse(const DevScene& s, V3 o, V3 d, float tmax, Hit& hit, int* st
     int overflow[kStackSize - kSmemStack];
     Walker<AnyHit, Count, Packed> w;
     w.init(o, d, tmax);
-    while (w.step(s, stack, stride, overflow, cnt)) {
+    const WalkScene ws{s.nodes, s.tris, &s};
+    while (w.step(ws, stack, stride, overflow, cnt)) {
     }
     if (w.tri >= 0) {
         hit.t = w.tmax;
@@ -288,9 +298,10 @@ struct AnyWalker4 {
             node = e;
         }
     }
-    PT_HD bool step(const DevScene& s, int* stack, int stride, int* overflow, TraversalCounters* cnt) {
+    // ws.nodes: the 4-wide BVH (8 float4 per node).
+    PT_HD bool step(const WalkScene& ws, int* stack, int stride, int* overflow, TraversalCounters* cnt) {
         if (!leaf_mode) {
-            const float4* n = s.nodes4 + 8 * node;
+            const float4* n = ws.nodes + 8 * node;
             const float4 lx = __ldg(n), ly = __ldg(n + 1), lz = __ldg(n + 2), hx = __ldg(n + 3), hy = __ldg(n + 4), hz = __ldg(n + 5);
             const int4 id = __ldg(reinterpret_cast<const int4*>(n + 6)), ct = __ldg(reinterpret_cast<const int4*>(n + 7));
             if (Count) cnt->nodes++;
@@ -314,12 +325,12 @@ struct AnyWalker4 {
         }
         if (leaf_mode) {
             const int i = ti;
-            const float4* g = s.tris + 3 * i;
+            const float4* g = ws.tris + 3 * i;
             float4 g0 = __ldg(g), g1 = __ldg(g + 1), g2 = __ldg(g + 2);
             float t, tu, tv;
             if (Count) cnt->tris++;
             if (tri_intersect(g0, g1, g2, o, d, tmax, t, tu, tv) &&
-                !((__float_as_int(g1.w) & 1) && alpha_passes(s, i, __float_as_int(g0.w), tu, tv))) {
+                !((__float_as_int(g1.w) & 1) && alpha_passes(*ws.scene, i, __float_as_int(g0.w), tu, tv))) {
                 hit = true;
                 done = true;
                 return false;
@@ -338,7 +349,8 @@ PT_HD bool occluded4(const DevScene& s, V3 o, V3 d, float tmax, int* stack, int 
     int overflow[kBvh4Stack - kSmemStack];
     AnyWalker4<Count, Packed> w;
     w.init(o, d, tmax);
-    while (w.step(s, stack, stride, overflow, cnt)) {
+    const WalkScene ws{s.nodes4, s.tris, &s};
+    while (w.step(ws, stack, stride, overflow, cnt)) {
     }
     return w.hit;
 }

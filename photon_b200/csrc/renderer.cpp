@@ -157,6 +157,7 @@ WfParams WavefrontEngine::params(const DevScene* scenes, int single, const DevVi
     p.wide_shadows = tuning_.wide_shadows;
     p.trace_refill = uint32_t(std::clamp(tuning_.trace_refill, 1, 32));
     p.shadow_refill = uint32_t(std::clamp(tuning_.shadow_refill, 1, 32));
+    p.walk_burst = uint32_t(std::clamp(tuning_.walk_burst, 1, 1 << 20));
     p.keys = keys_.ptr;
     p.hist = hist_.ptr;
     p.offsets = offsets_.ptr;
@@ -625,6 +626,15 @@ void Renderer::download_gbuffer(float* albedo4, float* nd4, size_t n) {
     PTW_CUDA(cudaStreamSynchronize(stream_));
 }
 
+void Renderer::download_accumulation(float* sums4, size_t n) {
+    size_t npix = size_t(width_) * size_t(height_);
+    if (n < npix) throw Error{PT_ERR_INVALID, "download_accumulation: buffer too small"};
+    if (npix == 0) return;
+    PTW_CUDA(cudaSetDevice(device_));
+    PTW_CUDA(cudaMemcpyAsync(sums4, accum_.ptr, npix * sizeof(float4), cudaMemcpyDeviceToHost, stream_));
+    PTW_CUDA(cudaStreamSynchronize(stream_));
+}
+
 void Renderer::stats(pt_stats* out) const {
     std::memset(out, 0, sizeof(*out));
     out->width = width_;
@@ -683,6 +693,8 @@ void Renderer::set_tuning(const pt_tuning& t) {
     if (t.trace_refill > 32 || t.shadow_refill > 32) throw Error{PT_ERR_INVALID, "trace_refill and shadow_refill must be in [1, 32]"};
     if (t.trace_refill > 0) cur.trace_refill = t.trace_refill;
     if (t.shadow_refill > 0) cur.shadow_refill = t.shadow_refill;
+    if (t.walk_burst > (1 << 20)) throw Error{PT_ERR_INVALID, "walk_burst must be in [1, 2^20]"};
+    if (t.walk_burst > 0) cur.walk_burst = t.walk_burst;
     engine_->set_tuning(cur);
 }
 
@@ -699,6 +711,7 @@ void Renderer::get_tuning(pt_tuning* t) const {
     t->wide_shadows = c.wide_shadows;
     t->trace_refill = c.trace_refill;
     t->shadow_refill = c.shadow_refill;
+    t->walk_burst = c.walk_burst;
 }
 
 // Coordinate descent over the knobs, one at a time, each candidate timed on the same probe (a view

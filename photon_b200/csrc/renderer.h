@@ -36,8 +36,9 @@ struct Tuning {
     int packed = 1;                // f32x2 slab tests
     int wide_shadows = 0;          // 1: shadow rays walk the 4-wide BVH (measured slower on the 262K scene)
     int tail_paths = kTailAuto;    // finish the last queued paths one thread each below this many (0: never)
-    int trace_refill = 16;         // a closest-hit warp claims new rays once fewer than this many lanes hold one
-    int shadow_refill = 16;        // the same for the shadow walk
+    int trace_refill = 24;         // a closest-hit warp claims new rays once fewer than this many lanes hold one
+    int shadow_refill = 24;        // the same for the shadow walk
+    int walk_burst = 16;           // walk steps a lane takes between two refill checks of its warp
 };
 
 // Runs wavefront passes over a table of views on one device stream. Owns the path pool, the
@@ -76,6 +77,9 @@ public:
     // the last begin().
     uint32_t tail_limit_in_use() const { return tail_limit_; }
     void set_work_total_async(const unsigned long long* pinned_value);
+    // Continuous mode: whether the next launches carry the ray-sort kernels (the tuning's sort_rays;
+    // the kernels still sort only iterations of at least kSortMinPaths paths).
+    void set_continuous_sorting(bool on) { cont_params_.sort_bits = on ? tuning_.sort_rays : 0; }
 
     const Counters& last() const { return last_; }
 
@@ -136,6 +140,7 @@ public:
     void download_image(float* rgb, size_t n);
     void download_display(uint32_t* out, size_t n);
     void download_gbuffer(float* albedo4, float* nd4, size_t n);
+    void download_accumulation(float* sums4, size_t n);
     uint32_t* display_buffer() const { return display_.ptr; }
     void stats(pt_stats* out) const;
     void set_tuning(const pt_tuning& t);

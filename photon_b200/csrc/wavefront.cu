@@ -184,14 +184,19 @@ __global__ void __launch_bounds__(256) k_generate(const __grid_constant__ WfPara
 // (one atomic per warp) and start them on the spot. A ray's walk, and so its result and its counts,
 // does not depend on the lane or the moment it starts, so every `refill` gives the same results;
 // refill = 1 claims only once all lanes have finished (32 consecutive rays at a time).
-// begin(i, w) initialises walker w from queue entry i and returns its scene; end(i, w) consumes the
-// finished walk. Count: tc.steps counts lane steps and warp_steps the loop's iterations.
-template <typename W, int Overflow, bool Count, typename Begin, typename End>
-__device__ __forceinline__ void walk_queue(uint32_t n, uint32_t* claim, uint32_t refill, int* stack, int stride, TraversalCounters& tc,
-                                           uint32_t& warp_steps, Begin begin, End end) {
+// The warp looks at its lanes only every `burst` steps: in between, each lane steps on its own, so
+// lanes in different phases of their walks (visiting nodes, testing a leaf's triangles) proceed as
+// separate groups whose load latencies overlap, instead of meeting at a warp-wide vote every step.
+// begin(i, w, ws) initialises walker w from queue entry i (and, unless Single, sets the lane's scene
+// arrays ws); end(i, w) consumes the finished walk. Single: every ray walks `uniform`, whose array
+// bases stay in registers for the whole loop. Count: tc.steps counts lane steps and warp_steps the
+// loop's iterations.
+template <typename W, int Overflow, bool Count, bool Single, typename Begin, typename End>
+__device__ __forceinline__ void walk_queue(uint32_t n, uint32_t* claim, uint32_t refill, uint32_t burst, int* stack, int stride,
+                                           const WalkScene& uniform, TraversalCounters& tc, uint32_t& warp_steps, Begin begin, End end) {
     int overflow[Overflow];
     W w;
-    const DevScene* s = nullptr;
+    WalkScene ws = uniform;
     uint32_t idx = 0;
     bool live = false, drained = false;
     const uint32_t lane = lane_id(), below = (1u << lane) - 1u;
@@ -207,27 +212,44 @@ __device__ __forceinline__ void walk_queue(uint32_t n, uint32_t* claim, uint32_t
                 const uint32_t r = base + uint32_t(__popc(idle & below));
                 if (r < n) {
                     idx = r;
-                    s = begin(r, w);
+                    begin(r, w, ws);
                     live = true;
                 }
             }
             act = __ballot_sync(kFull, live);
         }
         if (act == 0) break;
-        if (Count) warp_steps++;
+        uint32_t taken = 0;
         if (live) {
-            if (Count) tc.steps++;
-            if (!w.step(*s, stack, stride, overflow, &tc)) {
-                end(idx, w);
-                live = false;
+            while (taken < burst) {
+                taken++;
+                if (!w.step(Single ? uniform : ws, stack, stride, overflow, &tc)) {
+                    end(idx, w);
+                    live = false;
+                    break;
+                }
             }
+        }
+        if (Count) {
+            tc.steps += taken;
+            warp_steps += __reduce_max_sync(kFull, taken);  // the warp's steps in this burst: its busiest lane's
         }
     }
 }
 
+// The scene arrays of a launch whose views all use one scene (the renderer), or null arrays (the
+// server: each ray's scene comes from its view).
+__device__ __forceinline__ WalkScene single_walk_scene(const WfParams& P, bool wide) {
+    if (P.single_scene < 0) return WalkScene{nullptr, nullptr, nullptr};
+    const DevScene& s = P.scenes[P.single_scene];
+    return WalkScene{wide ? s.nodes4 : s.nodes, s.tris, &s};
+}
+
 // ---- trace: closest hit (traverse.h:140-142) -------------------------------------------------------
-template <bool Count, bool Packed>
-__global__ void __launch_bounds__(256) k_trace(const __grid_constant__ WfParams P) {
+// Single: every view of the launch uses scene slot P.single_scene (the renderer); otherwise each ray's
+// scene comes from its view (the server).
+template <bool Count, bool Packed, bool Single>
+__global__ void __maxnreg__(56) k_trace(const __grid_constant__ WfParams P) {
     extern __shared__ int smem_stack[];
     int* stack = smem_stack + threadIdx.x;
     Counters* c = P.ctr;
@@ -236,17 +258,24 @@ __global__ void __launch_bounds__(256) k_trace(const __grid_constant__ WfParams 
     TraversalCounters tc{0, 0, 0};
     uint32_t warp_steps = 0;
     using W = Walker<false, Count, Packed>;
-    walk_queue<W, kStackSize - kSmemStack, Count>(
-        n, &c->fetch[1], P.trace_refill, stack, blockDim.x, tc, warp_steps,
-        [&](uint32_t i, W& w) -> const DevScene* {
-            const float4 o4 = P.pb.o[p][i], d4 = P.pb.d[p][i];
-            const DevScene* s = &scene_for(P, P.single_scene >= 0 ? 0 : int(P.pb.id[p][i].x));
-            w.init(xyz(o4), xyz(d4), kInf);
-            return s;
-        },
-        [&](uint32_t i, const W& w) {
-            P.pb.hit[i] = w.tri >= 0 ? make_float4(w.tmax, __int_as_float(w.tri), w.u, w.v) : make_float4(kInf, __int_as_float(-1), 0.0f, 0.0f);
-        });
+    auto end = [&](uint32_t i, const W& w) {
+        P.pb.hit[i] = w.tri >= 0 ? make_float4(w.tmax, __int_as_float(w.tri), w.u, w.v) : make_float4(kInf, __int_as_float(-1), 0.0f, 0.0f);
+    };
+    const WalkScene uni = single_walk_scene(P, false);
+    if (Single) {
+        walk_queue<W, kStackSize - kSmemStack, Count, true>(
+            n, &c->fetch[1], P.trace_refill, P.walk_burst, stack, blockDim.x, uni, tc, warp_steps,
+            [&](uint32_t i, W& w, WalkScene&) { w.init(xyz(P.pb.o[p][i]), xyz(P.pb.d[p][i]), kInf); }, end);
+    } else {
+        walk_queue<W, kStackSize - kSmemStack, Count, false>(
+            n, &c->fetch[1], P.trace_refill, P.walk_burst, stack, blockDim.x, uni, tc, warp_steps,
+            [&](uint32_t i, W& w, WalkScene& ws) {
+                const DevScene& s = P.scenes[P.views[P.pb.id[p][i].x].scene];
+                ws = WalkScene{s.nodes, s.tris, &s};
+                w.init(xyz(P.pb.o[p][i]), xyz(P.pb.d[p][i]), kInf);
+            },
+            end);
+    }
     if (Count) {
         warp_add_u64(&c->node_visits, tc.nodes);
         warp_add_u64(&c->tri_tests, tc.tris);
@@ -615,7 +644,7 @@ __global__ void __launch_bounds__(256) k_tail(const __grid_constant__ WfParams P
 // resident warps than it loses to the tighter allocation (measured; the closest-hit walk does not).
 // Wide: the 4-wide BVH, used when every ray of the launch has it (a single scene that carries one);
 // otherwise the BVH2.
-template <bool Count, bool Packed, bool Wide>
+template <bool Count, bool Packed, bool Wide, bool Single>
 __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfParams P) {
     extern __shared__ int smem_stack[];
     int* stack = smem_stack + threadIdx.x;
@@ -624,12 +653,6 @@ __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfPar
     const uint32_t q = c->parity ^ 1u, n = c->shadow_count;
     TraversalCounters tc{0, 0, 0};
     uint32_t warp_steps = 0;
-    auto begin = [&](uint32_t i, auto& w) -> const DevScene* {
-        const float4 a = P.pb.sh0[i], b = P.pb.sh1[i];
-        const DevScene* s = &scene_for(P, P.single_scene >= 0 ? 0 : int(__float_as_uint(P.pb.sh2[i].w) & 0x7fffffffu));
-        w.init(xyz(a), xyz(b), a.w);
-        return s;
-    };
     // An unoccluded shadow ray adds its contribution to its path (or to its finished sample).
     auto deliver = [&](uint32_t i) {
         const float4 cc = P.pb.sh2[i];
@@ -647,18 +670,36 @@ __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfPar
             P.pb.lr[q][target] = l4;
         }
     };
-    if (Wide && P.single_scene >= 0 && P.scenes[P.single_scene].nodes4) {
+    auto init = [&](uint32_t i, auto& w) {
+        const float4 a = P.pb.sh0[i];
+        w.init(xyz(a), xyz(P.pb.sh1[i]), a.w);
+    };
+    if (Wide && Single && P.scenes[P.single_scene].nodes4) {
         using W4 = AnyWalker4<Count, Packed>;
-        walk_queue<W4, kBvh4Stack - kSmemStack, Count>(n, &c->fetch[3], P.shadow_refill, stack, blockDim.x, tc, warp_steps, begin,
-                                                       [&](uint32_t i, const W4& w) {
-                                                           if (!w.hit) deliver(i);
-                                                       });
+        walk_queue<W4, kBvh4Stack - kSmemStack, Count, true>(
+            n, &c->fetch[3], P.shadow_refill, P.walk_burst, stack, blockDim.x, single_walk_scene(P, true), tc, warp_steps,
+            [&](uint32_t i, W4& w, WalkScene&) { init(i, w); },
+            [&](uint32_t i, const W4& w) {
+                if (!w.hit) deliver(i);
+            });
     } else {
         using W = Walker<true, Count, Packed>;
-        walk_queue<W, kStackSize - kSmemStack, Count>(n, &c->fetch[3], P.shadow_refill, stack, blockDim.x, tc, warp_steps, begin,
-                                                      [&](uint32_t i, const W& w) {
-                                                          if (w.tri < 0) deliver(i);
-                                                      });
+        auto end = [&](uint32_t i, const W& w) {
+            if (w.tri < 0) deliver(i);
+        };
+        if (Single) {
+            walk_queue<W, kStackSize - kSmemStack, Count, true>(n, &c->fetch[3], P.shadow_refill, P.walk_burst, stack, blockDim.x, single_walk_scene(P, false),
+                                                                tc, warp_steps, [&](uint32_t i, W& w, WalkScene&) { init(i, w); }, end);
+        } else {
+            walk_queue<W, kStackSize - kSmemStack, Count, false>(
+                n, &c->fetch[3], P.shadow_refill, P.walk_burst, stack, blockDim.x, WalkScene{nullptr, nullptr, nullptr}, tc, warp_steps,
+                [&](uint32_t i, W& w, WalkScene& ws) {
+                    const DevScene& s = P.scenes[P.views[__float_as_uint(P.pb.sh2[i].w) & 0x7fffffffu].scene];
+                    ws = WalkScene{s.nodes, s.tris, &s};
+                    init(i, w);
+                },
+                end);
+        }
     }
     if (Count) {
         warp_add_u64(&c->shadow_node_visits, tc.nodes);
@@ -936,21 +977,24 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
     out->gen_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
     out->trace_block = trace_block;
     size_t smem = size_t(kSmemStack) * trace_block * sizeof(int);
-    const void* smem_kernels[] = {(const void*)k_trace<false, false>, (const void*)k_trace<false, true>, (const void*)k_trace<true, false>,
-                                  (const void*)k_trace<true, true>,
-                                  (const void*)k_shadow<false, false, false>, (const void*)k_shadow<false, true, false>,
-                                  (const void*)k_shadow<true, false, false>, (const void*)k_shadow<true, true, false>,
-                                  (const void*)k_shadow<false, false, true>, (const void*)k_shadow<false, true, true>,
-                                  (const void*)k_shadow<true, false, true>, (const void*)k_shadow<true, true, true>};
+#define PTW_TRACE_KERNELS(S) (const void*)k_trace<false, false, S>, (const void*)k_trace<false, true, S>, \
+                             (const void*)k_trace<true, false, S>, (const void*)k_trace<true, true, S>
+#define PTW_SHADOW_KERNELS(W, S) (const void*)k_shadow<false, false, W, S>, (const void*)k_shadow<false, true, W, S>, \
+                                 (const void*)k_shadow<true, false, W, S>, (const void*)k_shadow<true, true, W, S>
+    const void* smem_kernels[] = {PTW_TRACE_KERNELS(false), PTW_TRACE_KERNELS(true), PTW_SHADOW_KERNELS(false, false),
+                                  PTW_SHADOW_KERNELS(false, true), PTW_SHADOW_KERNELS(true, false), PTW_SHADOW_KERNELS(true, true)};
+#undef PTW_TRACE_KERNELS
+#undef PTW_SHADOW_KERNELS
     for (const void* k : smem_kernels) {
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
     }
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace<false, true>, trace_block, smem);
+    // Grids are sized for the heavier (multi-scene) variants, so that every variant's grid fits.
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace<false, true, false>, trace_block, smem);
     if (e != cudaSuccess) return e;
     out->trace_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
     out->shadow_block = trace_block;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shadow<false, true, true>, trace_block, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shadow<false, true, true, false>, trace_block, smem);
     if (e != cudaSuccess) return e;
     out->shadow_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
     out->shade_block = shade_block;
@@ -960,14 +1004,20 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
     return cudaSuccess;
 }
 
-template <bool Count, bool Packed>
+template <bool Count, bool Packed, bool Single>
 static void launch_traversals(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, size_t smem, bool shadow) {
     if (shadow) {
-        if (p.wide_shadows) k_shadow<Count, Packed, true><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
-        else k_shadow<Count, Packed, false><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
+        if (p.wide_shadows) k_shadow<Count, Packed, true, Single><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
+        else k_shadow<Count, Packed, false, Single><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
     } else {
-        k_trace<Count, Packed><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
+        k_trace<Count, Packed, Single><<<ls.trace_grid, ls.trace_block, smem, stream>>>(p);
     }
+}
+
+template <bool Count, bool Packed>
+static void launch_traversals(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, size_t smem, bool shadow) {
+    if (p.single_scene >= 0) launch_traversals<Count, Packed, true>(p, ls, stream, smem, shadow);
+    else launch_traversals<Count, Packed, false>(p, ls, stream, smem, shadow);
 }
 
 static void launch_traversal(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, size_t smem, bool shadow) {

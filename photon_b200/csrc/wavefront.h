@@ -89,6 +89,7 @@ struct WfParams {
     int wide_shadows;          // 1: shadow rays walk the 4-wide BVH where the scene has one
     uint32_t trace_refill;     // 1-32: a trace warp claims new rays once fewer of its lanes hold one
     uint32_t shadow_refill;    // the same for the shadow walk
+    uint32_t walk_burst;       // walk steps each lane takes between two looks at its warp (>= 1)
     int sort_material;         // 1: the shade kernel groups each block's paths by material class
     int sort_bits;             // > 0: sort continuing paths by direction octant + Morton origin cell
                                //      (this many bits per axis) before they are traced

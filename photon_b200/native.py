@@ -49,6 +49,7 @@ def _load():
         "pt_download_image": ([C.c_void_p, _f32p, C.c_size_t], C.c_int32),
         "pt_download_display": ([C.c_void_p, _u32p, C.c_size_t], C.c_int32),
         "pt_download_gbuffer": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t], C.c_int32),
+        "pt_download_accumulation": ([C.c_void_p, C.c_void_p, C.c_size_t], C.c_int32),
         "pt_display_buffer": ([C.c_void_p], C.c_void_p),
         "pt_get_stats": ([C.c_void_p, P(abi.Stats)], C.c_int32),
         "pt_renderer_stream": ([C.c_void_p], C.c_void_p),
@@ -223,6 +224,13 @@ class Renderer:
         _check(lib.pt_download_gbuffer(self.h, a.ctypes.data, nd.ctypes.data, s.width * s.height), self._err)
         return a, nd
 
+    def download_accumulation(self):
+        """Per-pixel sums (rgb radiance, squared luminance) of the samples rendered so far."""
+        s = self.stats()
+        a = np.zeros((s.height, s.width, 4), np.float32)
+        _check(lib.pt_download_accumulation(self.h, a.ctypes.data, s.width * s.height), self._err)
+        return a
+
     def stream(self):
         """The cudaStream_t (as an int) that orders all of this renderer's device work."""
         return lib.pt_renderer_stream(self.h)
@@ -236,7 +244,7 @@ class Renderer:
         return p
 
     def set_tuning(self, **kw):
-        t = abi.Tuning(0, 0, 0, -1, -1, -1, -1, -1, -1, 0, 0)
+        t = abi.Tuning(0, 0, 0, -1, -1, -1, -1, -1, -1, 0, 0, 0)
         for k, v in kw.items():
             setattr(t, k, v)
         _check(lib.pt_set_tuning(self.h, C.byref(t)), self._err)
@@ -343,8 +351,8 @@ def encode_png(rgba, level=6):
 class Server:
     """The request server (continuous batching over resident scenes)."""
 
-    def __init__(self, budget_bytes=0, device=0, path_capacity=0, max_active=0, device_wait_seconds=2.0):
-        cfg = abi.ServerConfig(device, budget_bytes, path_capacity, max_active, device_wait_seconds)
+    def __init__(self, budget_bytes=0, device=0, path_capacity=0, max_active=0, device_wait_seconds=2.0, sort_rays=0):
+        cfg = abi.ServerConfig(device, budget_bytes, path_capacity, max_active, device_wait_seconds, sort_rays)
         p = C.c_void_p()
         _check(lib.pt_server_create(C.byref(cfg), C.byref(p)), lib.pt_global_error)
         self.h = p
