@@ -280,8 +280,21 @@ def systems_sections(r, g, desc, rank):
         r.reset()
         r.render(v.camera, abi.RenderSettings(v.width, v.height, v.path, 1.0, abi.PT_TONEMAP_ACES, v.seed), v.spp)
     tp = time.perf_counter() - t0
+    # The autotuner on the view set (a copy scaled to 2^25 paths), then the same batch with its choice.
+    default_tuning = r.tuning()
+    t0 = time.perf_counter()
+    chosen, probe_default, probe_tuned = r.autotune_views(views, probe_samples=1 << 25)
+    tune_s = time.perf_counter() - t0
+    r.render_views(views)
+    t0 = time.perf_counter()
+    r.render_views(views)
+    tt = time.perf_counter() - t0
+    r.set_tuning(**default_tuning)
     out["batched"] = {"workload": "64 views of the 262K scene (seed 2)", "samples": total, "msamples_per_s": total / tb / 1e6,
-                      "plain_msamples_per_s": total / tp / 1e6, "batched_over_plain": tp / tb, "api": "pt_render_views"}
+                      "plain_msamples_per_s": total / tp / 1e6, "batched_over_plain": tp / tb, "api": "pt_render_views",
+                      "tuned": {"msamples_per_s": total / tt / 1e6, "tuned_over_default": tb / tt, "autotune_seconds": tune_s,
+                                "probe_msamples_per_s": {"default": probe_default / 1e6, "tuned": probe_tuned / 1e6},
+                                "chosen": chosen, "api": "pt_autotune_views"}}
     # The four resident scenes of the serving configuration (the larger two built on the device).
     scenes = [(native.box_scene(), None), (g, None), (native.terrain_scene(1 << 20, SEED), None), (native.terrain_scene(1 << 22, SEED), None)]
     built = []

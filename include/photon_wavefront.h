@@ -327,6 +327,14 @@ typedef struct pt_view {
  * the path pool, bounce iterations run as captured CUDA graphs. Results: pt_download_view. */
 int32_t pt_render_views(pt_renderer* r, const pt_view* views, int32_t n_views);
 int32_t pt_download_view(pt_renderer* r, int32_t view, float* rgb, size_t n);
+/* The autotuner for a batched view set (pt_render_views): the probe is the set itself with every
+ * view's resolution scaled by one factor to about `probe_samples` paths in all (0: 2^25). The chosen
+ * tuning stays with the renderer (its record for the resident scene), so later pt_render_views and
+ * pt_render calls use it; pt_get_tuning reads it back (pt_server_set_tuning applies it to a server). The
+ * results of the last pt_render_views stay downloadable. No counterpart in Photon (fixed 16x8 blocks,
+ * gpu_renderer.cu:60-80). */
+int32_t pt_autotune_views(pt_renderer* r, const pt_view* views, int32_t n_views, uint64_t probe_samples, pt_tuning* chosen,
+                          double* default_rate, double* tuned_rate);
 
 /* ---- SVGF on caller G-buffers (svgf.h:24-42) --------------------------------------------------
  * A denoiser session with its own history. Inputs are device pointers to width*height float4:
@@ -345,6 +353,10 @@ int32_t pt_svgf_run(pt_svgf* s, const float* color, const float* albedo, const f
  * beyond; 2 as 1 plus a strided tile (one residue class of x, y mod 8) for step 16; 3 strided tiles
  * for steps 1-16. Every mode gives the same output bit for bit. */
 int32_t pt_svgf_set_tma(pt_svgf* s, int32_t mode);
+/* Test hook for the TMA passes' bounded wait (no counterpart in Photon): with on = 1 they arm their
+ * tile barrier without issuing the tile copies and wait 2 us, so the wait runs out with no copy in
+ * flight; the timeout is reported as PT_ERR_CUDA by the next pt_svgf_run, and the frame is invalid. */
+int32_t pt_svgf_debug_tma_timeout(pt_svgf* s, int32_t on);
 const float* pt_svgf_variance(const pt_svgf* s);
 const char* pt_svgf_last_error(const pt_svgf* s);
 
@@ -414,6 +426,12 @@ typedef struct pt_request {
     int32_t width, height, spp;
     uint32_t seed;
     pt_path_options path;
+    /* display = 1: the finished image is also mapped for display on the device (the colour view of
+     * pt_display: exposure, tone map, sRGB, RGBA8) for pt_server_fetch_encoded's PNG; 0 (zero-filled
+     * requests): the float image only. */
+    int32_t display;
+    float exposure;
+    int32_t tonemap;           /* PT_TONEMAP_* */
 } pt_request;
 enum { PT_REQ_QUEUED = 0, PT_REQ_RUNNING = 1, PT_REQ_DONE = 2, PT_REQ_CANCELLED = 3, PT_REQ_FAILED = 4 };
 typedef struct pt_request_stats {
@@ -444,7 +462,21 @@ int32_t pt_server_wait(pt_server* s, uint64_t request_id, double timeout_s);
 /* Copies a finished request's average radiance (3 floats/pixel) and releases it. */
 int32_t pt_server_fetch(pt_server* s, uint64_t request_id, float* rgb, size_t n, pt_request_stats* st);
 int32_t pt_server_cancel(pt_server* s, uint64_t request_id);
+/* The headless image endpoint: a finished request's image encoded in a wire format, instead of raw
+ * floats. PT_IMAGE_PFM: the float rgb image in the format of Photon's save_pfm (image.cpp:88-96);
+ * PT_IMAGE_PNG: the request's display image (it must have been submitted with display = 1), RGBA8 as
+ * Photon's save_png writes a display buffer (image.cpp:84-86). With out == NULL only *length is set
+ * and the request stays (the encoding is kept for the next call); otherwise the bytes are copied
+ * (capacity >= *length, else PT_ERR_INVALID) and the request is consumed as by pt_server_fetch. */
+enum { PT_IMAGE_PFM = 0, PT_IMAGE_PNG = 1 };
+int32_t pt_server_fetch_encoded(pt_server* s, uint64_t request_id, int32_t format, uint8_t* out, size_t capacity, size_t* length);
 int32_t pt_server_get_stats(pt_server* s, pt_server_stats* out);
+/* Applies a tuning record (as pt_autotune / pt_autotune_views chose it for a scene) to the server's
+ * wavefront from its next batch: the material-sort window, ray-sort bits (at most the configured
+ * sort_rays), packed slab tests, 4-wide shadow BVH, walk refill and burst. Its pool size, block
+ * shapes, graph cadence and tail size are ignored (the pool is set by pt_server_config). Images do not
+ * change with any of them. Thread-safe. */
+int32_t pt_server_set_tuning(pt_server* s, const pt_tuning* t);
 /* Test hook (host-side fault injection): the next `count` device allocations of request buffers
  * fail, so the affected requests end in PT_REQ_FAILED without touching the GPU. */
 int32_t pt_server_debug_fail_allocations(pt_server* s, int32_t count);

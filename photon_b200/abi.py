@@ -25,6 +25,7 @@ PT_TONEMAP_LINEAR, PT_TONEMAP_ACES, PT_TONEMAP_REINHARD = 0, 1, 2
  PT_DISPLAY_HEATMAP) = range(6)
 PT_REQ_QUEUED, PT_REQ_RUNNING, PT_REQ_DONE, PT_REQ_CANCELLED, PT_REQ_FAILED = range(5)
 PT_GEN_BOX, PT_GEN_TERRAIN = 0, 1
+PT_IMAGE_PFM, PT_IMAGE_PNG = 0, 1
 
 
 class Vec2(C.Structure):
@@ -190,7 +191,8 @@ class ServerConfig(C.Structure):
 
 class Request(C.Structure):
     _fields_ = [("scene_id", C.c_int32), ("camera", Camera), ("width", C.c_int32), ("height", C.c_int32),
-                ("spp", C.c_int32), ("seed", C.c_uint32), ("path", PathOptions)]
+                ("spp", C.c_int32), ("seed", C.c_uint32), ("path", PathOptions), ("display", C.c_int32), ("exposure", C.c_float),
+                ("tonemap", C.c_int32)]
 
 
 class RequestStats(C.Structure):

@@ -224,6 +224,12 @@ int32_t pt_autotune(pt_renderer* r, const pt_camera* camera, const pt_render_set
     PT_RENDERER_CALL(r, r->r->autotune(*camera, *settings, spp, probe_samples, chosen, default_rate, tuned_rate));
 }
 
+int32_t pt_autotune_views(pt_renderer* r, const pt_view* views, int32_t n_views, uint64_t probe_samples, pt_tuning* chosen,
+                          double* default_rate, double* tuned_rate) {
+    if (!views || n_views <= 0) return PT_ERR_INVALID;
+    PT_RENDERER_CALL(r, r->r->autotune_views(views, n_views, probe_samples, chosen, default_rate, tuned_rate));
+}
+
 int32_t pt_get_tuning(const pt_renderer* r, pt_tuning* t) {
     if (!r || !r->r || !t) return PT_ERR_INVALID;
     r->r->get_tuning(t);
@@ -293,6 +299,11 @@ int32_t pt_svgf_run(pt_svgf* s, const float* color, const float* albedo, const f
 int32_t pt_svgf_set_tma(pt_svgf* s, int32_t mode) {
     if (!s) return PT_ERR_INVALID;
     return guarded(&server_error, [&] { s->s->set_tma(mode); });
+}
+
+int32_t pt_svgf_debug_tma_timeout(pt_svgf* s, int32_t on) {
+    if (!s) return PT_ERR_INVALID;
+    return guarded(&server_error, [&] { s->s->set_tma_timeout_test(on != 0); });
 }
 
 const float* pt_svgf_variance(const pt_svgf* s) { return s ? s->s->variance() : nullptr; }
@@ -365,6 +376,16 @@ int32_t pt_server_get_stats(pt_server* s, pt_server_stats* out) {
 int32_t pt_server_debug_fail_allocations(pt_server* s, int32_t count) {
     if (!s || count < 0) return PT_ERR_INVALID;
     return guarded(&server_error, [&] { s->s->inject_allocation_failures(count); });
+}
+
+int32_t pt_server_fetch_encoded(pt_server* s, uint64_t request_id, int32_t format, uint8_t* out, size_t capacity, size_t* length) {
+    if (!s || !length || (format != PT_IMAGE_PFM && format != PT_IMAGE_PNG)) return PT_ERR_INVALID;
+    return guarded(&server_error, [&] { s->s->fetch_encoded(request_id, format, out, capacity, length); });
+}
+
+int32_t pt_server_set_tuning(pt_server* s, const pt_tuning* t) {
+    if (!s || !t) return PT_ERR_INVALID;
+    return guarded(&server_error, [&] { s->s->set_tuning(*t); });
 }
 
 int32_t pt_server_debug_fail_finishing(pt_server* s, int32_t count) {

@@ -8,6 +8,7 @@
 #include <string>
 #include <vector>
 
+#include "image_io.h"
 #include "photon_wavefront.h"
 
 namespace {
@@ -27,6 +28,10 @@ void put_chunk(std::vector<uint8_t>& out, const char type[4], const uint8_t* dat
     uLong crc = crc32(0L, out.data() + start, uInt(4 + n));
     put_u32be(out, uint32_t(crc));
 }
+
+}  // namespace
+
+namespace ptw {
 
 // PFM: "PF\n<w> <h>\n-1.0\n" then float rgb rows, bottom row first, little endian.
 std::vector<uint8_t> encode_pfm(const float* rgb, int w, int h) {
@@ -68,6 +73,10 @@ bool encode_png(const uint32_t* rgba, int w, int h, int level, std::vector<uint8
     return true;
 }
 
+}  // namespace ptw
+
+namespace {
+
 int32_t copy_out(const std::vector<uint8_t>& v, uint8_t* out, size_t cap, size_t* len) {
     if (len) *len = v.size();
     if (!out) return PT_OK;  // size query
@@ -85,6 +94,9 @@ int32_t write_file(const char* path, const std::vector<uint8_t>& v) {
 }
 
 }  // namespace
+
+using ptw::encode_pfm;
+using ptw::encode_png;
 
 extern "C" {
 

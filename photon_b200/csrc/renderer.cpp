@@ -245,6 +245,26 @@ void WavefrontEngine::begin(const DevScene* scenes, const DevView* views, int n_
     cont_params_ = params(scenes, -1, views, n_views, false);
 }
 
+void WavefrontEngine::update_scheduling(const Tuning& t) {
+    if (t.sort_rays > 0 && hist_.count < (size_t(8) << (3 * t.sort_rays)))
+        throw Error{PT_ERR_INVALID, "sort_rays above the bits the running wavefront was sized for"};
+    tuning_.sort_by_material = t.sort_by_material;
+    tuning_.sort_rays = t.sort_rays;
+    tuning_.packed = t.packed;
+    tuning_.wide_shadows = t.wide_shadows;
+    tuning_.trace_refill = t.trace_refill;
+    tuning_.shadow_refill = t.shadow_refill;
+    tuning_.walk_burst = t.walk_burst;
+    const WfParams fresh = params(cont_params_.scenes, cont_params_.single_scene, cont_params_.views, cont_params_.num_views, false);
+    cont_params_.sort_material = fresh.sort_material;
+    cont_params_.packed = fresh.packed;
+    cont_params_.wide_shadows = fresh.wide_shadows;
+    cont_params_.trace_refill = fresh.trace_refill;
+    cont_params_.shadow_refill = fresh.shadow_refill;
+    cont_params_.walk_burst = fresh.walk_burst;
+    if (cont_params_.sort_bits > 0) cont_params_.sort_bits = tuning_.sort_rays;
+}
+
 void WavefrontEngine::set_views(const DevView* views, int n_views) {
     cont_params_.views = views;
     cont_params_.num_views = n_views;
@@ -714,10 +734,76 @@ void Renderer::get_tuning(pt_tuning* t) const {
     t->walk_burst = c.walk_burst;
 }
 
-// Coordinate descent over the knobs, one at a time, each candidate timed on the same probe (a view
-// of the camera at a reduced resolution so that it holds about probe_samples paths). Every probe
-// runs twice and keeps the faster time, after a warm-up render with the candidate (graph capture and
-// buffer growth are not timed).
+// Coordinate descent over the knobs, one at a time, each candidate timed on the same probe view set.
+// Every probe runs twice and keeps the faster time, after a warm-up render with the candidate (graph
+// capture and buffer growth are not timed). A knob moves only for a gain above 1%. The probe renders
+// into the batched-view buffers, whose previous contents are put back afterwards.
+void Renderer::tune_on(const std::vector<pt_view>& probe, pt_tuning* chosen, double* default_rate, double* tuned_rate) {
+    uint64_t samples = 0;
+    for (const pt_view& v : probe) samples += uint64_t(v.width) * uint64_t(v.height) * uint64_t(v.spp);
+    if (samples == 0) throw Error{PT_ERR_INVALID, "autotune: the probe has no samples"};
+    std::vector<pt_view> saved_views;
+    std::vector<DeviceBuffer<float4>> saved_accum, saved_pass;
+    saved_views.swap(batch_views_);
+    saved_accum.swap(batch_accum_);
+    saved_pass.swap(batch_pass_);
+    auto restore = [&]() {
+        batch_views_.swap(saved_views);
+        batch_accum_.swap(saved_accum);
+        batch_pass_.swap(saved_pass);
+    };
+    try {
+        auto time_probe = [&]() {
+            render_views(probe.data(), int(probe.size()));  // warm-up (graph capture, buffer growth)
+            float best = 1e30f;
+            for (int k = 0; k < 2; k++) {
+                render_views(probe.data(), int(probe.size()));
+                best = std::min(best, last_ms_);
+            }
+            return double(samples) / (double(best) / 1000.0);
+        };
+        Tuning base = engine_->tuning();
+        engine_->set_tuning(base);
+        double best_rate = time_probe();
+        if (default_rate) *default_rate = best_rate;
+        Tuning best = base;
+        auto try_knob = [&](auto setter, std::initializer_list<int> values) {
+            Tuning start = best;
+            for (int val : values) {
+                Tuning t = start;
+                setter(t, val);
+                engine_->set_tuning(t);
+                double rate = time_probe();
+                if (rate > best_rate * 1.01) {
+                    best_rate = rate;
+                    best = t;
+                }
+            }
+            engine_->set_tuning(best);
+        };
+        try_knob([](Tuning& t, int v) { t.path_capacity = v; }, {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24});
+        try_knob([](Tuning& t, int v) { t.trace_block = v; }, {64, 128, 256});
+        try_knob([](Tuning& t, int v) { t.shade_block = v; }, {64, 128, 256});
+        try_knob([](Tuning& t, int v) { t.sort_by_material = v; }, {0, 1, 2, 4});
+        try_knob([](Tuning& t, int v) { t.graph_bounces = v; }, {2, 4, 8});
+        try_knob([](Tuning& t, int v) { t.sort_rays = v; }, {0, 3, 4, 5});
+        try_knob([](Tuning& t, int v) { t.tail_paths = v; }, {0, 1 << 16, 1 << 17, 1 << 18, 1 << 20});
+        try_knob([](Tuning& t, int v) { t.wide_shadows = v; }, {0, 1});
+        try_knob([](Tuning& t, int v) { t.trace_refill = v; }, {1, 8, 16, 24, 32});
+        try_knob([](Tuning& t, int v) { t.shadow_refill = v; }, {1, 8, 16, 24, 32});
+        try_knob([](Tuning& t, int v) { t.walk_burst = v; }, {4, 8, 16, 32, 64});
+        engine_->set_tuning(best);
+        if (tuned_rate) *tuned_rate = best_rate;
+        if (chosen) get_tuning(chosen);
+    } catch (...) {
+        restore();
+        throw;
+    }
+    restore();
+}
+
+// The single-view autotuner: the probe is the camera's view at a reduced resolution that holds about
+// probe_samples paths.
 void Renderer::autotune(const pt_camera& cam, const pt_render_settings& rs, int spp, uint64_t probe_samples, pt_tuning* chosen,
                         double* default_rate, double* tuned_rate) {
     if (!scene_.ready()) throw Error{PT_ERR_NO_SCENE, "autotune before upload"};
@@ -732,48 +818,26 @@ void Renderer::autotune(const pt_camera& cam, const pt_render_settings& rs, int 
     v.spp = spp;
     v.seed = rs.seed;
     v.path = rs.path;
-    uint64_t samples = uint64_t(v.width) * uint64_t(v.height) * uint64_t(spp);
-    std::vector<pt_view> saved_views = batch_views_;
-    auto time_probe = [&]() {
-        render_views(&v, 1);  // warm-up (graph capture, buffer growth)
-        float best = 1e30f;
-        for (int k = 0; k < 2; k++) {
-            render_views(&v, 1);
-            best = std::min(best, last_ms_);
-        }
-        return double(samples) / (double(best) / 1000.0);
-    };
-    Tuning base = engine_->tuning();
-    engine_->set_tuning(base);
-    double best_rate = time_probe();
-    if (default_rate) *default_rate = best_rate;
-    Tuning best = base;
-    auto try_knob = [&](auto setter, std::initializer_list<int> values) {
-        Tuning start = best;
-        for (int val : values) {
-            Tuning t = start;
-            setter(t, val);
-            engine_->set_tuning(t);
-            double rate = time_probe();
-            if (rate > best_rate * 1.01) {
-                best_rate = rate;
-                best = t;
-            }
-        }
-        engine_->set_tuning(best);
-    };
-    try_knob([](Tuning& t, int v) { t.path_capacity = v; }, {1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24});
-    try_knob([](Tuning& t, int v) { t.trace_block = v; }, {64, 128, 256});
-    try_knob([](Tuning& t, int v) { t.shade_block = v; }, {64, 128, 256});
-    try_knob([](Tuning& t, int v) { t.sort_by_material = v; }, {0, 1, 2, 4});
-    try_knob([](Tuning& t, int v) { t.graph_bounces = v; }, {2, 4, 8});
-    try_knob([](Tuning& t, int v) { t.sort_rays = v; }, {0, 3, 4, 5});
-    try_knob([](Tuning& t, int v) { t.tail_paths = v; }, {0, 1 << 16, 1 << 17, 1 << 18, 1 << 20});
-    try_knob([](Tuning& t, int v) { t.wide_shadows = v; }, {0, 1});
-    engine_->set_tuning(best);
-    batch_views_ = saved_views;
-    if (tuned_rate) *tuned_rate = best_rate;
-    if (chosen) get_tuning(chosen);
+    tune_on({v}, chosen, default_rate, tuned_rate);
+}
+
+// The batched form's autotuner: the probe is the view set itself with every view's resolution scaled
+// by one factor so that the set holds about probe_samples paths (spp, cameras and options kept).
+void Renderer::autotune_views(const pt_view* views, int n, uint64_t probe_samples, pt_tuning* chosen, double* default_rate,
+                              double* tuned_rate) {
+    if (!scene_.ready()) throw Error{PT_ERR_NO_SCENE, "autotune before upload"};
+    if (n <= 0 || !views) throw Error{PT_ERR_INVALID, "autotune: no views"};
+    if (probe_samples == 0) probe_samples = uint64_t(1) << 25;
+    double full = 0;
+    for (int i = 0; i < n; i++) full += double(views[i].width) * double(views[i].height) * double(views[i].spp);
+    if (full <= 0) throw Error{PT_ERR_INVALID, "autotune: the views have no samples"};
+    double scale = std::min(1.0, std::sqrt(double(probe_samples) / full));
+    std::vector<pt_view> probe(views, views + n);
+    for (pt_view& v : probe) {
+        v.width = std::max(8, int(v.width * scale));
+        v.height = std::max(8, int(v.height * scale));
+    }
+    tune_on(probe, chosen, default_rate, tuned_rate);
 }
 
 void Renderer::trace_primary(const pt_camera& cam, int w, int h, uint32_t frame, uint32_t seed, float* hits4) {

@@ -80,6 +80,11 @@ public:
     // Continuous mode: whether the next launches carry the ray-sort kernels (the tuning's sort_rays;
     // the kernels still sort only iterations of at least kSortMinPaths paths).
     void set_continuous_sorting(bool on) { cont_params_.sort_bits = on ? tuning_.sort_rays : 0; }
+    // Continuous mode: takes the knobs of `t` that only change what the next launches are given
+    // (material-sort window, ray-sort bits up to those the buffers were sized for, packed slab tests,
+    // 4-wide shadow BVH, walk refill and burst). Pool size, block shapes, graph cadence and the tail
+    // stay as they were set before begin().
+    void update_scheduling(const Tuning& t);
 
     const Counters& last() const { return last_; }
 
@@ -147,6 +152,7 @@ public:
     void get_tuning(pt_tuning* t) const;
     void autotune(const pt_camera& cam, const pt_render_settings& rs, int spp, uint64_t probe_samples, pt_tuning* chosen,
                   double* default_rate, double* tuned_rate);
+    void autotune_views(const pt_view* views, int n, uint64_t probe_samples, pt_tuning* chosen, double* default_rate, double* tuned_rate);
 
     void trace_primary(const pt_camera& cam, int w, int h, uint32_t frame, uint32_t seed, float* hits4);
     void light_picks(const pt_camera& cam, const pt_render_settings& rs, uint32_t frame, int32_t* picks4);
@@ -165,6 +171,7 @@ private:
     void fill_view(DevView& v, const pt_camera& cam, int w, int h, int spp, uint32_t seed, const pt_path_options& po,
                    uint32_t frame0) const;
     void render_pass_set(std::vector<DevView>& views, int spp_total, std::vector<int>& spp_each, std::vector<uint32_t>& frame0);
+    void tune_on(const std::vector<pt_view>& probe, pt_tuning* chosen, double* default_rate, double* tuned_rate);
 
     int device_;
     cudaStream_t stream_ = nullptr;

@@ -18,7 +18,10 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstring>
+
+#include "image_io.h"
 
 namespace ptw {
 
@@ -45,6 +48,7 @@ Server::Server(const pt_server_config& cfg) : cfg_(cfg), device_(cfg.device) {
     t.path_capacity = cfg.path_capacity > 0 ? cfg.path_capacity : (1 << 24);
     if (cfg.sort_rays < -1 || cfg.sort_rays > 6) throw Error{PT_ERR_INVALID, "sort_rays must be in [-1, 6]"};
     t.sort_rays = cfg.sort_rays > 0 ? cfg.sort_rays : (cfg.sort_rays == 0 ? 4 : 0);
+    created_sort_rays_ = t.sort_rays;
     engine_->set_tuning(t);
     engine_->reserve_paths(uint64_t(t.path_capacity));
     pool_bytes_ = engine_->device_bytes();
@@ -107,6 +111,7 @@ Server::~Server() {
 double Server::now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count(); }
 
 size_t Server::request_bytes(const pt_request& r) const {
+    // (The display image, when asked for, goes into the sample buffer after the float image.)
     size_t npix = size_t(r.width) * size_t(r.height);
     return npix * size_t(r.spp) * sizeof(float4) + npix * sizeof(float4) + sizeof(DevView) + sizeof(unsigned long long);
 }
@@ -149,6 +154,8 @@ uint64_t Server::submit(const pt_request& r) {
     if (r.path.max_depth < 0 || r.path.max_depth > 65535) throw Error{PT_ERR_INVALID, "request: max_depth must be in [0, 65535]"};
     if (uint64_t(r.width) * uint64_t(r.height) * uint64_t(r.spp) >= (uint64_t(1) << 32))
         throw Error{PT_ERR_INVALID, "request: more than 2^32 samples"};
+    if (r.display != 0 && (r.display != 1 || r.tonemap < 0 || r.tonemap > 2 || !std::isfinite(r.exposure)))
+        throw Error{PT_ERR_INVALID, "request: display must be 0 or 1, with a tone map in [0, 2] and a finite exposure"};
     std::lock_guard<std::mutex> g(mu_);
     if (r.scene_id < 0 || r.scene_id >= int(scenes_.size())) throw Error{PT_ERR_NOT_FOUND, "request: unknown scene"};
     size_t need = request_bytes(r);
@@ -202,6 +209,7 @@ void Server::fetch(uint64_t id, float* rgb, size_t n, pt_request_stats* st) {
     if (it == requests_.end() || it->second->fetched) throw Error{PT_ERR_NOT_FOUND, "unknown request"};
     Request& r = *it->second;
     if (r.state == PT_REQ_QUEUED || r.state == PT_REQ_RUNNING) throw Error{PT_ERR_INVALID, "request not finished"};
+    if (r.encoding) throw Error{PT_ERR_INVALID, "fetch: another call is encoding this request"};
     if (st) {
         st->submit_s = r.submit_s;
         st->admit_s = r.admit_s;
@@ -219,6 +227,48 @@ void Server::fetch(uint64_t id, float* rgb, size_t n, pt_request_stats* st) {
     r.fetched = true;
     if (r.batch_refs == 0) requests_.erase(it);  // else the loop erases it after its last batch
     if (state == PT_REQ_CANCELLED) throw Error{PT_ERR_CANCELLED, "request cancelled"};
+}
+
+void Server::fetch_encoded(uint64_t id, int format, uint8_t* out, size_t capacity, size_t* length) {
+    std::unique_lock<std::mutex> lk(mu_);
+    auto it = requests_.find(id);
+    if (it == requests_.end() || it->second->fetched) throw Error{PT_ERR_NOT_FOUND, "unknown request"};
+    Request& r = *it->second;
+    if (r.state == PT_REQ_QUEUED || r.state == PT_REQ_RUNNING) throw Error{PT_ERR_INVALID, "request not finished"};
+    if (r.state == PT_REQ_CANCELLED) throw Error{PT_ERR_CANCELLED, "request cancelled"};
+    if (r.state == PT_REQ_FAILED) throw Error{PT_ERR_CUDA, "request failed: " + r.error};
+    if (r.encoding) throw Error{PT_ERR_INVALID, "fetch: another call is encoding this request"};
+    if (format == PT_IMAGE_PNG && !r.req.display) throw Error{PT_ERR_INVALID, "PNG: the request was not submitted with display = 1"};
+    if (r.encoded_format != format) {
+        // Encoding (PNG: zlib) takes milliseconds: it runs outside the lock. The request cannot go
+        // away meanwhile: only a fetch consumes it, and fetches refuse a request being encoded.
+        r.encoding = true;
+        const float* rgb = r.result;
+        const int w = r.req.width, h = r.req.height;
+        lk.unlock();
+        std::vector<uint8_t> enc;
+        bool ok = true;
+        try {
+            if (format == PT_IMAGE_PFM) enc = encode_pfm(rgb, w, h);
+            else ok = encode_png(reinterpret_cast<const uint32_t*>(rgb + 3 * size_t(w) * size_t(h)), w, h, 6, enc);
+        } catch (const std::bad_alloc&) {
+            ok = false;
+        }
+        lk.lock();
+        r.encoding = false;
+        if (!ok) throw Error{PT_ERR_ALLOC, "fetch: encoding failed"};
+        r.encoded = std::move(enc);
+        r.encoded_format = format;
+    }
+    *length = r.encoded.size();
+    if (!out) return;  // a size query keeps the request
+    if (capacity < r.encoded.size()) throw Error{PT_ERR_INVALID, "fetch: buffer too small"};
+    std::memcpy(out, r.encoded.data(), r.encoded.size());
+    pinned_release(r.result, r.result_bytes);
+    r.result = nullptr;
+    r.encoded = std::vector<uint8_t>();
+    r.fetched = true;
+    if (r.batch_refs == 0) requests_.erase(it);  // else the loop erases it after its last batch
 }
 
 void Server::cancel(uint64_t id) {
@@ -254,6 +304,29 @@ void Server::inject_allocation_failures(int n) {
 }
 
 void Server::inject_finishing_failures(int n) { inject_finish_failures_.store(n); }
+
+void Server::set_tuning(const pt_tuning& t) {
+    std::lock_guard<std::mutex> g(mu_);
+    Tuning cur = tuning_pending_ ? pending_tuning_ : engine_->tuning();
+    if (t.sort_by_material >= 0) {
+        if (t.sort_by_material > 4) throw Error{PT_ERR_INVALID, "sort_by_material must be in [0, 4]"};
+        cur.sort_by_material = t.sort_by_material;
+    }
+    if (t.sort_rays >= 0) {
+        if (t.sort_rays > created_sort_rays_) throw Error{PT_ERR_INVALID, "sort_rays above the server's configured sort_rays"};
+        cur.sort_rays = t.sort_rays;
+    }
+    if (t.packed >= 0) cur.packed = t.packed ? 1 : 0;
+    if (t.wide_shadows >= 0) cur.wide_shadows = t.wide_shadows ? 1 : 0;
+    if (t.trace_refill > 32 || t.shadow_refill > 32) throw Error{PT_ERR_INVALID, "trace_refill and shadow_refill must be in [1, 32]"};
+    if (t.walk_burst > (1 << 20)) throw Error{PT_ERR_INVALID, "walk_burst must be in [1, 2^20]"};
+    if (t.trace_refill > 0) cur.trace_refill = t.trace_refill;
+    if (t.shadow_refill > 0) cur.shadow_refill = t.shadow_refill;
+    if (t.walk_burst > 0) cur.walk_burst = t.walk_burst;
+    pending_tuning_ = cur;
+    tuning_pending_ = true;
+    cv_work_.notify_all();
+}
 
 // Called with the lock held: drops the references of a completed batch's snapshot, erasing the
 // requests that were fetched meanwhile.
@@ -422,6 +495,10 @@ void Server::loop() {
             }
             append_chunks();
             if (scenes_dirty_) upload_scene_table();
+            if (tuning_pending_ && engine_started_) {
+                engine_->update_scheduling(pending_tuning_);
+                tuning_pending_ = false;
+            }
             Batch& B = batch_[cur];
             Batch& P = batch_[cur ^ 1];
             if (views_uploaded_ < views_.size()) {
@@ -532,6 +609,23 @@ void Server::loop() {
                     float* rgb = reinterpret_cast<float*>(r->sample_out);
                     PTW_CUDA(wf_resolve(r->accum, npix, 1.0f / float(r->req.spp), true, rgb, fin_stream_));
                     r->result_bytes = size_t(npix) * 3 * sizeof(float);
+                    if (r->req.display) {
+                        // The colour view of pt_display on the summed samples, into the rest of the
+                        // sample buffer (it holds spp >= 1 float4 per pixel: room for 12 + 4 bytes).
+                        DisplayParams dp{};
+                        dp.w = r->req.width;
+                        dp.h = r->req.height;
+                        dp.mode = PT_DISPLAY_COLOR;
+                        dp.exposure = r->req.exposure;
+                        dp.tonemap = r->req.tonemap;
+                        dp.samples = float(r->req.spp);
+                        dp.inv_samples = 1.0f / float(r->req.spp);
+                        dp.max_depth = 1.0f;
+                        dp.heat_scale = 1.0f / 160.0f;
+                        uint32_t* rgba = reinterpret_cast<uint32_t*>(rgb + 3 * size_t(npix));
+                        PTW_CUDA(wf_display(dp, r->accum, nullptr, nullptr, nullptr, nullptr, nullptr, rgba, fin_stream_));
+                        r->result_bytes += size_t(npix) * sizeof(uint32_t);
+                    }
                     r->result = pinned_acquire(r->result_bytes);
                     PTW_CUDA(cudaMemcpyAsync(r->result, rgb, r->result_bytes, cudaMemcpyDeviceToHost, fin_stream_));
                     release_buffers(*r, fin_stream_);

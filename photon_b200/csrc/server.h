@@ -26,6 +26,7 @@ public:
     int32_t poll(uint64_t id);
     void wait(uint64_t id, double timeout_s);
     void fetch(uint64_t id, float* rgb, size_t n, pt_request_stats* st);
+    void fetch_encoded(uint64_t id, int format, uint8_t* out, size_t capacity, size_t* length);
     void cancel(uint64_t id);
     void stats(pt_server_stats* out);
 
@@ -34,6 +35,8 @@ public:
     // Host-side fault injection for tests: the next `n` finishing steps fail (an error thrown right
     // after a finished request has been queued for its read-back, as a failing CUDA call would).
     void inject_finishing_failures(int n);
+    // A tuning record (pt_server_set_tuning): its scheduling knobs apply from the next batch.
+    void set_tuning(const pt_tuning& t);
 
 private:
     struct Request {
@@ -56,8 +59,12 @@ private:
         std::string error;
         float4* sample_out = nullptr;  // stream-ordered allocations from the server's memory pool
         float4* accum = nullptr;
-        float* result = nullptr;  // rgb (pinned, from the server's staging pool), filled when done
+        float* result = nullptr;  // rgb (pinned, from the server's staging pool), filled when done; with
+                                  // req.display the RGBA8 display image follows the 3 * pixels floats
         size_t result_bytes = 0;
+        std::vector<uint8_t> encoded;  // the image in encoded_format, kept by a size query
+        int encoded_format = -1;
+        bool encoding = false;         // a fetch_encoded call is encoding it outside the lock
     };
 
     void loop();
@@ -131,6 +138,9 @@ private:
     size_t pool_bytes_ = 0;
     bool engine_started_ = false;
     int inject_failures_ = 0;
+    bool tuning_pending_ = false;  // under mu_: pending_tuning_ waits for the loop
+    int created_sort_rays_ = 0;    // the ray-sort bits the wavefront's buffers are sized for
+    Tuning pending_tuning_;
     std::atomic<int> inject_finish_failures_{0};  // read by the loop outside the lock
 
     pt_server_stats st_{};

@@ -300,7 +300,9 @@ __global__ void __launch_bounds__(128) k_atrous(const float4* __restrict__ edge,
 //   (float lane, x mod e, x / e, y mod e, y / e) whose box is lanes 4, 1, 16 + 4r, 1, 16 + 4r.
 constexpr int kTmaTile = 16;
 constexpr int kTmaPasses = 5;   // steps 1, 2, 4, 8, 16 may be staged
-constexpr unsigned long long kTmaWaitNs = 200000000ull;  // 0.2 s: far beyond any tile load
+constexpr unsigned long long kTmaWaitNs = 200000000ull;    // 0.2 s: far beyond any tile load
+constexpr unsigned long long kTmaDrainNs = 2000000000ull;  // after a timeout: the copies' last chance to land
+constexpr unsigned long long kTmaTestWaitNs = 2000ull;     // the test mode's waits (no copy is issued)
 
 __host__ __device__ constexpr int tma_box_side(int r) { return kTmaTile + 4 * r; }
 size_t tma_smem_bytes(int r) { return 2 * size_t(tma_box_side(r)) * size_t(tma_box_side(r)) * sizeof(float4) + 16; }
@@ -323,11 +325,11 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-// Waits for phase 0 of the tile barrier for at most kTmaWaitNs.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar) {
+// Waits for phase 0 of the tile barrier for at most `limit_ns`.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned long long limit_ns) {
     const unsigned long long t0 = global_ns();
     while (!mbar_try_wait(bar, 0))
-        if (global_ns() - t0 > kTmaWaitNs) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     return true;
 }
 
@@ -337,7 +339,7 @@ __global__ void __launch_bounds__(kTmaTile * kTmaTile) k_atrous_tma(const __grid
                                                                     const float4* __restrict__ src, const float4* __restrict__ edge,
                                                                     int w, int h, int e, int r, float phi_color, float phi_normal,
                                                                     float phi_depth, float4* __restrict__ dst, AtrousEpilogue ep,
-                                                                    int* status) {
+                                                                    int* status, int test_no_copy) {
     extern __shared__ __align__(128) float4 tile_smem[];
     const int n = tma_box_side(r);  // box side in grid cells
     float4* t_src = tile_smem;
@@ -351,9 +353,13 @@ __global__ void __launch_bounds__(kTmaTile * kTmaTile) k_atrous_tma(const __grid
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    // Test mode (test_no_copy): the barrier is armed for the tiles but no copy is issued, so the wait
+    // below runs out with nothing in flight and the timeout path is exercised without any risk.
     if (leader) {
         const uint32_t bytes = uint32_t(2 * n * n * sizeof(float4));
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+    }
+    if (leader && !test_no_copy) {
         const int bx = cx0 - 2 * r, by = cy0 - 2 * r;
         if (Rank == 2) {
             // Innermost coordinate in floats: 4 * bx, a multiple of 4 floats = 16 bytes.
@@ -380,10 +386,14 @@ __global__ void __launch_bounds__(kTmaTile * kTmaTile) k_atrous_tma(const __grid
                 : "memory");
         }
     }
-    if (!mbar_wait_bounded(bar)) {
-        // The copies did not land in time: report, give them one more bounded wait, leave.
+    if (!mbar_wait_bounded(bar, test_no_copy ? kTmaTestWaitNs : kTmaWaitNs)) {
+        // The tiles did not land in time: report it (the host then fails the call and discards the
+        // frame) and wait once more, ten times longer, for the copies in flight, so that the block
+        // does not leave while they may still write its shared memory. Copies of valid coordinates
+        // into this block's own tile complete unless the device itself has failed; only then can the
+        // second wait also run out, and the block leaves so that the kernel ends.
         if (leader) atomicOr(status, 1);
-        mbar_wait_bounded(bar);
+        mbar_wait_bounded(bar, test_no_copy ? kTmaTestWaitNs : kTmaDrainNs);
         return;
     }
     const int tx = int(threadIdx.x), ty = int(threadIdx.y);
@@ -479,6 +489,7 @@ struct TmaPlan {
     const CUtensorMap* maps;
     const TmaPass* passes;  // [kTmaPasses]
     int* status;
+    int test_no_copy;       // the timeout test mode (SvgfDenoiser::set_tma_timeout_test)
 };
 
 template <bool FromPhoton>
@@ -514,10 +525,12 @@ void denoise(const Frame5& in5, const SvgfFrame& in, const PrevCamera& pc, int w
             const CUtensorMap& me = tma.maps[it];
             if (tp.rank == 2)
                 k_atrous_tma<2><<<tgrid, dim3(kTmaTile, kTmaTile), tma_smem_bytes(tp.r), stream>>>(
-                    ms, me, bufs[src], edge, w, h, tp.e, tp.r, s.phi_color, s.phi_normal, s.phi_depth, bufs[1 - src], ep, tma.status);
+                    ms, me, bufs[src], edge, w, h, tp.e, tp.r, s.phi_color, s.phi_normal, s.phi_depth, bufs[1 - src], ep, tma.status,
+                    tma.test_no_copy);
             else
                 k_atrous_tma<5><<<tgrid, dim3(kTmaTile, kTmaTile), tma_smem_bytes(tp.r), stream>>>(
-                    ms, me, bufs[src], edge, w, h, tp.e, tp.r, s.phi_color, s.phi_normal, s.phi_depth, bufs[1 - src], ep, tma.status);
+                    ms, me, bufs[src], edge, w, h, tp.e, tp.r, s.phi_color, s.phi_normal, s.phi_depth, bufs[1 - src], ep, tma.status,
+                    tma.test_no_copy);
         } else {
             k_atrous<<<grid, block, 0, stream>>>(edge, w, h, 1 << it, s.phi_color, s.phi_normal, s.phi_depth, bufs[src], bufs[1 - src],
                                                  ep);
@@ -698,7 +711,7 @@ void SvgfDenoiser::run(const float* color, const float* albedo, const float* nd,
     std::memcpy(pc.c, &prev, sizeof(pc.c));
     History hist{prev_illum_.ptr, prev_moments_.ptr, prev_edge_.ptr};
     AtrousEpilogue hist_out{prev_illum_.ptr, prev_moments_.ptr, prev_edge_.ptr, illum_.ptr, moments_.ptr, nullptr, nullptr, nullptr, nullptr};
-    TmaPlan plan{maps_ok_ ? maps_.data() : nullptr, passes_, status_dev_};
+    TmaPlan plan{maps_ok_ ? maps_.data() : nullptr, passes_, status_dev_, tma_test_ ? 1 : 0};
     denoise<true>(in5, SvgfFrame{}, pc, w_, h_, has_history_, hist, edge_.ptr, hist_out, illum_.ptr, moments_.ptr, filter_[0].ptr,
                   filter_[1].ptr, s, output, plan, stream_);
     has_history_ = true;
@@ -713,7 +726,7 @@ void SvgfDenoiser::run_frame(const float* color, const float* albedo, const floa
                  reinterpret_cast<const float4*>(edge), reinterpret_cast<const float4*>(motion)};
     History hist{prev_illum_.ptr, prev_moments_.ptr, prev_edge_.ptr};
     AtrousEpilogue hist_out{prev_illum_.ptr, prev_moments_.ptr, prev_edge_.ptr, illum_.ptr, moments_.ptr, nullptr, nullptr, nullptr, nullptr};
-    TmaPlan plan{maps_ok_ ? maps_.data() : nullptr, passes_, status_dev_};
+    TmaPlan plan{maps_ok_ ? maps_.data() : nullptr, passes_, status_dev_, tma_test_ ? 1 : 0};
     denoise<false>(Frame5{}, in, PrevCamera{}, w_, h_, has_history_, hist, edge_.ptr, hist_out, illum_.ptr, moments_.ptr, filter_[0].ptr,
                    filter_[1].ptr, s, output, plan, stream_);
     has_history_ = true;
@@ -768,7 +781,7 @@ void svgf_run_noalloc(int device, int w, int h, const float* color, const float*
         // Without history the temporal step reads nothing from earlier calls, and every scratch
         // element a kernel reads was written earlier in this call: nothing needs clearing.
         denoise<true>(in5, SvgfFrame{}, PrevCamera{}, w, h, false, History{}, edge, AtrousEpilogue{}, illum, moments, f0, f1, s, output,
-                      TmaPlan{nullptr, nullptr, nullptr}, stream);
+                      TmaPlan{nullptr, nullptr, nullptr, 0}, stream);
     } catch (...) {
         cudaSetDevice(previous);
         throw;

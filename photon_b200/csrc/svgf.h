@@ -28,6 +28,9 @@ public:
     // shared-memory tiles for some steps (see tma_passes_for_mode in svgf.cu).
     void set_tma(int mode);
     bool tma_active() const { return maps_ok_; }
+    // Test hook: the TMA passes arm their tile barrier without issuing the copies and wait 2 us, so
+    // their bounded wait runs out with no copy in flight; the next call reports PT_ERR_CUDA.
+    void set_tma_timeout_test(bool on) { tma_test_ = on; }
     void reset() { has_history_ = false; }
     // Svgf::run (svgf.cu:238-255): inputs and output are device float4 buffers of width*height in
     // Photon's SvgfInput layout (colour, albedo, normal + depth, position + material, emission).
@@ -54,6 +57,7 @@ private:
     int w_ = 0, h_ = 0;
     bool has_history_ = false;
     int tma_mode_ = 1;
+    bool tma_test_ = false;
     bool maps_ok_ = false;
     std::vector<CUtensorMap> maps_;    // [edge, filter 0, filter 1][pass]
     TmaPass passes_[5];

@@ -60,6 +60,10 @@ def _load():
         "pt_get_tuning": ([C.c_void_p, P(abi.Tuning)], C.c_int32),
         "pt_autotune": ([C.c_void_p, P(abi.Camera), P(abi.RenderSettings), C.c_int32, C.c_uint64, P(abi.Tuning),
                          P(C.c_double), P(C.c_double)], C.c_int32),
+        "pt_autotune_views": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_uint64, P(abi.Tuning), P(C.c_double), P(C.c_double)],
+                              C.c_int32),
+        "pt_server_set_tuning": ([C.c_void_p, P(abi.Tuning)], C.c_int32),
+        "pt_server_fetch_encoded": ([C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p, C.c_size_t, P(C.c_size_t)], C.c_int32),
         "pt_trace_primary": ([C.c_void_p, P(abi.Camera), C.c_int32, C.c_int32, C.c_uint32, C.c_uint32, _f32p], C.c_int32),
         "pt_light_picks_primary": ([C.c_void_p, P(abi.Camera), P(abi.RenderSettings), C.c_uint32, _i32p], C.c_int32),
         "pt_heatmap": ([C.c_void_p, P(abi.Camera), C.c_int32, C.c_int32, _f32p], C.c_int32),
@@ -73,6 +77,7 @@ def _load():
         "pt_svgf_variance": ([C.c_void_p], C.c_void_p),
         "pt_svgf_last_error": ([C.c_void_p], C.c_char_p),
         "pt_svgf_set_tma": ([C.c_void_p, C.c_int32], C.c_int32),
+        "pt_svgf_debug_tma_timeout": ([C.c_void_p, C.c_int32], C.c_int32),
         "pt_rebuild_lights": ([C.c_void_p, P(abi.LightUpdate)], C.c_int32),
         "pt_encode_pfm": ([C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, P(C.c_size_t)], C.c_int32),
         "pt_encode_png": ([C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_size_t, P(C.c_size_t)], C.c_int32),
@@ -256,6 +261,15 @@ class Renderer:
         _check(lib.pt_autotune(self.h, C.byref(cam), C.byref(rs), spp, probe_samples, C.byref(t), C.byref(d), C.byref(b)), self._err)
         return {n: getattr(t, n) for n, _ in abi.Tuning._fields_}, d.value, b.value
 
+    def autotune_views(self, views, probe_samples=0):
+        """Runs the autotuner on a batched view set; returns (chosen tuning dict, default rate, tuned
+        rate) in samples/s of the scaled-down probe."""
+        arr = (abi.View * len(views))(*views)
+        t = abi.Tuning()
+        d, b = C.c_double(), C.c_double()
+        _check(lib.pt_autotune_views(self.h, arr, len(views), probe_samples, C.byref(t), C.byref(d), C.byref(b)), self._err)
+        return {n: getattr(t, n) for n, _ in abi.Tuning._fields_}, d.value, b.value
+
     def tuning(self):
         t = abi.Tuning()
         _check(lib.pt_get_tuning(self.h, C.byref(t)), self._err)
@@ -306,6 +320,10 @@ class Svgf:
     def set_tma(self, mode):
         """0 global loads, 1-3 TMA-staged tiles (pt_svgf_set_tma)."""
         _check(lib.pt_svgf_set_tma(self.h, int(mode)), lambda: lib.pt_svgf_last_error(self.h))
+
+    def debug_tma_timeout(self, on):
+        """Test hook: the TMA passes' tile wait runs out with no copy issued (pt_svgf_debug_tma_timeout)."""
+        _check(lib.pt_svgf_debug_tma_timeout(self.h, 1 if on else 0), lambda: lib.pt_svgf_last_error(self.h))
 
     def variance_ptr(self):
         return lib.pt_svgf_variance(self.h)
@@ -366,8 +384,8 @@ class Server:
         _check(lib.pt_server_add_scene(self.h, C.byref(desc), C.byref(sid)), self._err)
         return sid.value
 
-    def submit(self, scene_id, cam, w, h, spp, seed=0, path=None):
-        req = abi.Request(scene_id, cam, w, h, spp, seed, path or abi.path_options())
+    def submit(self, scene_id, cam, w, h, spp, seed=0, path=None, display=False, exposure=1.0, tonemap=abi.PT_TONEMAP_ACES):
+        req = abi.Request(scene_id, cam, w, h, spp, seed, path or abi.path_options(), 1 if display else 0, exposure, tonemap)
         rid = C.c_uint64()
         _check(lib.pt_server_submit(self.h, C.byref(req), C.byref(rid)), self._err)
         return rid.value
@@ -389,6 +407,19 @@ class Server:
     def cancel(self, rid):
         _check(lib.pt_server_cancel(self.h, rid), self._err)
 
+    def encoded_size(self, rid, fmt):
+        """Size of the request's image in `fmt` (abi.PT_IMAGE_*); the request stays."""
+        n = C.c_size_t()
+        _check(lib.pt_server_fetch_encoded(self.h, rid, fmt, None, 0, C.byref(n)), self._err)
+        return n.value
+
+    def fetch_encoded(self, rid, fmt):
+        """The request's image encoded as PFM or PNG (bytes); consumes the request."""
+        n = self.encoded_size(rid, fmt)
+        buf = (C.c_uint8 * n)()
+        _check(lib.pt_server_fetch_encoded(self.h, rid, fmt, buf, n, C.byref(C.c_size_t())), self._err)
+        return bytes(buf)
+
     def stats(self):
         s = abi.ServerStats()
         _check(lib.pt_server_get_stats(self.h, C.byref(s)), self._err)
@@ -396,6 +427,13 @@ class Server:
 
     def fail_allocations(self, n):
         _check(lib.pt_server_debug_fail_allocations(self.h, n), self._err)
+
+    def set_tuning(self, **kw):
+        """Applies tuning knobs (pt_server_set_tuning); unnamed knobs keep their values."""
+        t = abi.Tuning(0, 0, 0, -1, -1, -1, -1, -1, -1, 0, 0, 0)
+        for k, v in kw.items():
+            setattr(t, k, v)
+        _check(lib.pt_server_set_tuning(self.h, C.byref(t)), self._err)
 
     def fail_finishing(self, n):
         _check(lib.pt_server_debug_fail_finishing(self.h, n), self._err)

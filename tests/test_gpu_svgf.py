@@ -199,3 +199,38 @@ def test_tma_staged_passes_equal_direct_loads(torch_cuda, w, h, iterations):
     for staged in outs[1:]:
         for a, b in zip(staged, outs[0]):
             assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_tma_tile_wait_timeout_is_reported(torch_cuda):
+    """The TMA-staged passes wait for their tiles with a bounded wait. A test hook arms each tile's
+    barrier without issuing its copies and shortens the wait to 2 us, so every staged pass's wait runs
+    out with nothing in flight (nothing can land late). The call after that frame reports PT_ERR_CUDA;
+    with the hook off, the same session denoises again, bit-identical to a fresh session."""
+    torch = torch_cuda
+    w, h = 96, 64
+    cams, gbufs, keep = _frames("cornell", w, h, 2)
+    settings = abi.svgf_settings()
+    dev = {n: torch.from_numpy(a).cuda() for n, a in gbufs[0].items()}
+    out = torch.zeros((h, w, 4), dtype=torch.float32, device="cuda")
+
+    def run(sv):
+        sv.run(dev["color"].data_ptr(), dev["albedo"].data_ptr(), dev["normal_depth"].data_ptr(), dev["position"].data_ptr(),
+               dev["emission"].data_ptr(), cams[0], settings, out.data_ptr())
+        torch.cuda.synchronize()
+        return out.cpu().numpy()
+
+    fresh = native.Svgf(w, h)
+    want = run(fresh)
+    fresh.close()
+    sv = native.Svgf(w, h)
+    sv.set_tma(1)  # steps 1-8 staged through TMA tiles
+    sv.debug_tma_timeout(True)
+    run(sv)  # every staged pass times out here; the flag is read by the next call
+    with pytest.raises(native.PhotonError) as e:
+        run(sv)
+    assert e.value.code == abi.PT_ERR_CUDA
+    sv.debug_tma_timeout(False)
+    sv.reset()
+    got = run(sv)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    sv.close()

@@ -289,3 +289,91 @@ def test_server_survives_immediate_fetches_of_many_small_requests(server_scenes)
     r.render(cam, abi.RenderSettings(16, 16, abi.path_options(), 1.0, abi.PT_TONEMAP_ACES, 205), 1)
     assert np.array_equal(served.view(np.uint32), r.download_image().view(np.uint32))
     r.close()
+
+
+def test_autotuner_record_is_used_by_batches_and_the_server():
+    """pt_autotune_views tunes on a scaled-down copy of a view set: its probe rate with the chosen
+    tuning is no lower than with the default, the record stays with the renderer (pt_get_tuning) and
+    the last batch stays downloadable; the views render bit-identically with it; and a server given the
+    record (pt_server_set_tuning) renders a request bit-identically to a server left at its defaults."""
+    desc, camf, keep = scenes.scene("terrain")
+    sizes = [(160, 90, 4, 1), (96, 54, 16, 2), (200, 120, 1, 3), (64, 64, 8, 4)]
+    views = []
+    for k, (w, h, spp, seed) in enumerate(sizes):
+        cam = camf(w / h)
+        cam.position.z += 0.2 * k
+        views.append(_view(cam, w, h, spp, seed, depth=12))
+    r = native.Renderer()
+    r.upload(desc)
+    r.render_views(views)
+    before = [r.download_view(k, v.width, v.height) for k, v in enumerate(views)]
+    chosen, default_rate, tuned_rate = r.autotune_views(views, probe_samples=1 << 18)
+    assert tuned_rate >= default_rate > 0
+    assert r.tuning() == chosen
+    for k, v in enumerate(views):  # the autotuner's probes did not overwrite the last batch
+        assert np.array_equal(r.download_view(k, v.width, v.height).view(np.uint32), before[k].view(np.uint32))
+    r.render_views(views)
+    for k, v in enumerate(views):
+        assert np.array_equal(r.download_view(k, v.width, v.height).view(np.uint32), before[k].view(np.uint32)), f"view {k}"
+    c1, d1, t1 = r.autotune(views[0].camera, abi.RenderSettings(160, 90, views[0].path, 1.0, abi.PT_TONEMAP_ACES, 1), 4,
+                            probe_samples=1 << 16)
+    assert t1 >= d1 > 0
+    r.close()
+    knobs = ("sort_by_material", "sort_rays", "packed", "wide_shadows", "trace_refill", "shadow_refill", "walk_burst")
+    images = []
+    for record in (None, {k: chosen[k] for k in knobs}):
+        s = native.Server(budget_bytes=8 << 30, path_capacity=1 << 18)
+        sid = s.add_scene(desc)
+        if record:
+            record["sort_rays"] = min(record["sort_rays"], 4)
+            s.set_tuning(**record)
+        rid = s.submit(sid, views[1].camera, 96, 54, 16, seed=2, path=abi.path_options(max_depth=12))
+        s.wait(rid, 60)
+        img, _ = s.fetch(rid, 96, 54)
+        images.append(img)
+        s.close()
+    assert np.array_equal(images[0].view(np.uint32), images[1].view(np.uint32))
+    assert np.array_equal(images[0].view(np.uint32), before[1].view(np.uint32))
+
+
+def test_server_serves_encoded_images(server_scenes):
+    """The headless image endpoint: a finished request fetched as PFM is the byte stream of the float
+    image in Photon's save_pfm format, and fetched as PNG the colour view of its samples (exposure, tone
+    map, sRGB, RGBA8, mapped on the device at finishing). Both equal the plain renderer's image and
+    display buffer of the same request. A size query keeps the request; PNG needs display = 1."""
+    from test_image_io import _decode_png
+    _, (tdesc, tcam, tkeep) = server_scenes
+    s = native.Server(budget_bytes=8 << 30, path_capacity=1 << 18)
+    sid = s.add_scene(tdesc)
+    w, h, spp, seed = 96, 54, 8, 21
+    cam = tcam(w / h)
+    path = abi.path_options(max_depth=12)
+    kw = dict(seed=seed, path=path, display=True, exposure=1.5, tonemap=abi.PT_TONEMAP_REINHARD)
+    a, b = s.submit(sid, cam, w, h, spp, **kw), s.submit(sid, cam, w, h, spp, **kw)
+    plain_only = s.submit(sid, cam, w, h, spp, seed=seed, path=path)
+    for rid in (a, b, plain_only):
+        s.wait(rid, 60)
+    n = s.encoded_size(a, abi.PT_IMAGE_PFM)
+    assert s.encoded_size(a, abi.PT_IMAGE_PFM) == n == len(f"PF\n{w} {h}\n-1.0\n") + w * h * 12
+    pfm = s.fetch_encoded(a, abi.PT_IMAGE_PFM)
+    with pytest.raises(native.PhotonError) as e:  # consumed
+        s.poll(a)
+    assert e.value.code == abi.PT_ERR_NOT_FOUND
+    png = _decode_png(s.fetch_encoded(b, abi.PT_IMAGE_PNG))
+    with pytest.raises(native.PhotonError) as e:
+        s.fetch_encoded(plain_only, abi.PT_IMAGE_PNG)
+    assert e.value.code == abi.PT_ERR_INVALID
+    img_c, _ = s.fetch(plain_only, w, h)
+    s.close()
+    r = native.Renderer()
+    r.upload(tdesc)
+    r.resize(w, h)
+    rs = abi.RenderSettings(w, h, path, 1.5, abi.PT_TONEMAP_REINHARD, seed)
+    r.render(cam, rs, spp)
+    img = r.download_image()
+    r.display(rs, abi.PT_DISPLAY_COLOR)
+    disp = r.download_display()
+    r.close()
+    assert np.array_equal(img.view(np.uint32), img_c.view(np.uint32))
+    assert pfm == native.encode_pfm(img)
+    assert np.array_equal(png, disp)
