@@ -329,10 +329,19 @@ def systems_sections(r, g, desc, rank):
                                  "scenes of 36 / 262,144 / 1,048,576 / 4,194,304 triangles, 150 GB budget",
                      "served": served, "plain": plain, "budget_bytes": budget,
                      "served_over_plain": served["msamples_per_s"] / plain["msamples_per_s"]}
+    # Eight real-time SVGF sessions served by the same server alongside the same stream (sessions as
+    # a request class sharing the path pool), and the same sessions on renderers of their own.
+    server = native.Server(budget_bytes=budget)
+    sids = [server.add_scene(d) for d in descs]
+    serving.run_served(server, warm)
+    both = serving.run_sessions_served(server, sids[1], desc, 8, 120, 1600, 900,
+                                       stream=workloads.request_stream(list(zip(sids, descs)), SERVED_REQUESTS, SERVED_RATE, seed=7))
+    server.close()
     from photon_b200 import sessions
-    out["sessions"] = dict(sessions.run_sessions(desc, 8, 120, 1600, 900),
-                           workload="8 real-time SVGF sessions, 120-frame orbits (0.5 deg/frame) of the 262K scene, 1600x900, 1 spp",
-                           api="pt_render_denoised")
+    out["sessions"] = dict(both, workload="8 real-time SVGF sessions (120-frame orbits, 0.5 deg/frame, of the 262K scene, 1600x900, "
+                                          "1 spp) served by the request server alongside the served stream above",
+                           api="pt_server_open_session / pt_server_submit_frame",
+                           standalone=dict(sessions.run_sessions(desc, 8, 120, 1600, 900), api="pt_render_denoised, one renderer per session"))
     return out
 
 

@@ -419,6 +419,9 @@ typedef struct pt_server_config {
     int32_t sort_rays;         /* ray sorting of iterations of at least 2,097,152 paths, bits per axis of the
                                   origin cell (1-6); 0: the default (4, while that many paths are
                                   pending); -1: off */
+    int64_t reserve_bytes;     /* device memory reserved up front for request buffers (0: min(32 GiB, half
+                                  the free memory, what the budget leaves beside the path pool);
+                                  negative: none, the pool grows on demand) */
 } pt_server_config;
 typedef struct pt_request {
     int32_t scene_id;
@@ -446,6 +449,8 @@ typedef struct pt_server_stats {
     uint64_t device_bytes_in_use, budget_bytes;
     int32_t active, queued, scenes;
     double busy_seconds;
+    double device_seconds;     /* device time of the bounce-iteration batches (CUDA events), for the busy fraction */
+    uint64_t batches;          /* batches of bounce iterations launched */
 } pt_server_stats;
 int32_t pt_server_create(const pt_server_config* cfg, pt_server** out);
 void pt_server_destroy(pt_server* s);
@@ -471,6 +476,22 @@ int32_t pt_server_cancel(pt_server* s, uint64_t request_id);
 enum { PT_IMAGE_PFM = 0, PT_IMAGE_PNG = 1 };
 int32_t pt_server_fetch_encoded(pt_server* s, uint64_t request_id, int32_t format, uint8_t* out, size_t capacity, size_t* length);
 int32_t pt_server_get_stats(pt_server* s, pt_server_stats* out);
+/* Real-time SVGF sessions served beside the requests (GpuRenderer::render_denoised, gpu_renderer.cu:
+ * 379-401, as a request class of the server). A session holds a G-buffer and a denoiser history on
+ * the server's device (counted against its budget). Each frame is one path per pixel of `camera`
+ * (sample index = the session's frame number, seed and path options from `settings`), whose first
+ * vertex writes the G-buffer and the denoiser's records (reprojection into `previous`), rendered in
+ * the shared path pool with every other request in flight, then denoised by SVGF (temporal, variance,
+ * `atrous_iterations` a-trous passes) with the session's history. The result is the denoised image:
+ * pt_server_poll / wait / fetch take the returned request id as for any request; it equals the image
+ * of the same frame sequence through pt_render_denoised. A session's frames are rendered one at a
+ * time in submission order (a frame waits for its predecessor's denoise); they are not held back by
+ * max_active. Closing a session cancels its frames still waiting; one on the device finishes first. */
+int32_t pt_server_open_session(pt_server* s, int32_t scene_id, int32_t width, int32_t height, const pt_svgf_settings* svgf,
+                               int32_t* session_id);
+int32_t pt_server_submit_frame(pt_server* s, int32_t session_id, const pt_camera* camera, const pt_camera* previous,
+                               const pt_render_settings* settings, uint64_t* request_id);
+int32_t pt_server_close_session(pt_server* s, int32_t session_id);
 /* Applies a tuning record (as pt_autotune / pt_autotune_views chose it for a scene) to the server's
  * wavefront from its next batch: the material-sort window, ray-sort bits (at most the configured
  * sort_rays), packed slab tests, 4-wide shadow BVH, walk refill and burst. Its pool size, block

@@ -186,7 +186,8 @@ class View(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("budget_bytes", C.c_uint64), ("path_capacity", C.c_int32),
-                ("max_active", C.c_int32), ("device_wait_seconds", C.c_double), ("sort_rays", C.c_int32)]
+                ("max_active", C.c_int32), ("device_wait_seconds", C.c_double), ("sort_rays", C.c_int32),
+                ("reserve_bytes", C.c_int64)]
 
 
 class Request(C.Structure):
@@ -204,7 +205,8 @@ class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("cancelled", C.c_uint64),
                 ("rejected", C.c_uint64), ("samples_done", C.c_uint64), ("bounce_iterations", C.c_uint64),
                 ("device_bytes_in_use", C.c_uint64), ("budget_bytes", C.c_uint64),
-                ("active", C.c_int32), ("queued", C.c_int32), ("scenes", C.c_int32), ("busy_seconds", C.c_double)]
+                ("active", C.c_int32), ("queued", C.c_int32), ("scenes", C.c_int32), ("busy_seconds", C.c_double),
+                ("device_seconds", C.c_double), ("batches", C.c_uint64)]
 
 
 def path_options(max_depth=8, rr_depth=3, clamp=0.0, nee=1):

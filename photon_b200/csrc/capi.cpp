@@ -383,6 +383,23 @@ int32_t pt_server_fetch_encoded(pt_server* s, uint64_t request_id, int32_t forma
     return guarded(&server_error, [&] { s->s->fetch_encoded(request_id, format, out, capacity, length); });
 }
 
+int32_t pt_server_open_session(pt_server* s, int32_t scene_id, int32_t width, int32_t height, const pt_svgf_settings* svgf,
+                               int32_t* session_id) {
+    if (!s || !svgf || !session_id) return PT_ERR_INVALID;
+    return guarded(&server_error, [&] { *session_id = s->s->open_session(scene_id, width, height, *svgf); });
+}
+
+int32_t pt_server_submit_frame(pt_server* s, int32_t session_id, const pt_camera* camera, const pt_camera* previous,
+                               const pt_render_settings* settings, uint64_t* request_id) {
+    if (!s || !camera || !previous || !settings || !request_id) return PT_ERR_INVALID;
+    return guarded(&server_error, [&] { *request_id = s->s->submit_frame(session_id, *camera, *previous, *settings); });
+}
+
+int32_t pt_server_close_session(pt_server* s, int32_t session_id) {
+    if (!s) return PT_ERR_INVALID;
+    return guarded(&server_error, [&] { s->s->close_session(session_id); });
+}
+
 int32_t pt_server_set_tuning(pt_server* s, const pt_tuning* t) {
     if (!s || !t) return PT_ERR_INVALID;
     return guarded(&server_error, [&] { s->s->set_tuning(*t); });

@@ -63,6 +63,23 @@ Server::Server(const pt_server_config& cfg) : cfg_(cfg), device_(cfg.device) {
     PTW_CUDA(cudaMemPoolCreate(&mem_pool_, &props));
     uint64_t keep = ~uint64_t(0);  // freed request buffers stay in the pool for the next admissions
     PTW_CUDA(cudaMemPoolSetAttribute(mem_pool_, cudaMemPoolAttrReleaseThreshold, &keep));
+    // Reserve the pool's working set now: growing it while requests run maps memory on the loop's
+    // thread between batches, and the device idles meanwhile (a fresh server's first saturating
+    // stream ran at 0.60 of the device's time, the same stream again at 0.89). Up to 32 GiB, half the
+    // free memory, and what the budget leaves beside the path pool.
+    {
+        size_t free_b = 0, total_b = 0;
+        PTW_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        size_t reserve = std::min<size_t>(size_t(32) << 30, free_b / 2);
+        if (cfg.budget_bytes) reserve = std::min<size_t>(reserve, cfg.budget_bytes > pool_bytes_ ? cfg.budget_bytes - pool_bytes_ : 0);
+        if (cfg.reserve_bytes > 0) reserve = std::min<size_t>(size_t(cfg.reserve_bytes), free_b / 2);
+        if (cfg.reserve_bytes < 0) reserve = 0;
+        if (reserve >= (size_t(1) << 20)) {
+            void* p = nullptr;
+            if (cudaMallocFromPoolAsync(&p, reserve, mem_pool_, stream_) == cudaSuccess) PTW_CUDA(cudaFreeAsync(p, stream_));
+            else cudaGetLastError();  // no reservation: the pool grows on demand
+        }
+    }
     PTW_CUDA(cudaStreamCreateWithFlags(&fin_stream_, cudaStreamNonBlocking));
     for (Batch& b : batch_) {
         PTW_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&b.ctr), sizeof(Counters), cudaHostAllocDefault));
@@ -90,17 +107,18 @@ Server::~Server() {
     for (auto& kv : requests_) release_buffers(*kv.second, stream_);
     for (Finishing& f : finishing_) cudaEventDestroy(f.ev);
     for (auto& kv : requests_)
-        if (kv.second->result) cudaFreeHost(kv.second->result);
+        if (kv.second->result) cudaFreeAsync(kv.second->result, stream_);
     cudaStreamSynchronize(stream_);
     for (Batch& b : batch_) {
         cudaFreeHost(b.ctr);
         cudaFreeHost(b.work_total);
         if (b.done) cudaFreeHost(b.done);
+        if (b.views) cudaFreeHost(b.views);
         cudaEventDestroy(b.ev);
         cudaEventDestroy(b.ev_start);
     }
-    for (auto& kv : pinned_free_) cudaFreeHost(kv.second);
     requests_.clear();
+    sessions_.clear();
     engine_.reset();
     scenes_.clear();
     if (mem_pool_) cudaMemPoolDestroy(mem_pool_);
@@ -203,13 +221,25 @@ void Server::wait(uint64_t id, double timeout_s) {
     }
 }
 
+// Copies part of a finished request's device result into caller memory, on the calling thread (with
+// the server's device current for the copy, the caller's restored after it).
+void Server::read_result(const Request& r, void* dst, size_t offset, size_t bytes) {
+    int previous = 0;
+    PTW_CUDA(cudaGetDevice(&previous));
+    PTW_CUDA(cudaSetDevice(device_));
+    cudaError_t e = cudaMemcpyAsync(dst, reinterpret_cast<const char*>(r.result) + offset, bytes, cudaMemcpyDeviceToHost, cudaStreamPerThread);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread);
+    cudaSetDevice(previous);
+    PTW_CUDA(e);
+}
+
 void Server::fetch(uint64_t id, float* rgb, size_t n, pt_request_stats* st) {
-    std::lock_guard<std::mutex> g(mu_);
+    std::unique_lock<std::mutex> g(mu_);
     auto it = requests_.find(id);
     if (it == requests_.end() || it->second->fetched) throw Error{PT_ERR_NOT_FOUND, "unknown request"};
     Request& r = *it->second;
     if (r.state == PT_REQ_QUEUED || r.state == PT_REQ_RUNNING) throw Error{PT_ERR_INVALID, "request not finished"};
-    if (r.encoding) throw Error{PT_ERR_INVALID, "fetch: another call is encoding this request"};
+    if (r.reading) throw Error{PT_ERR_INVALID, "fetch: another call is reading this request"};
     if (st) {
         st->submit_s = r.submit_s;
         st->admit_s = r.admit_s;
@@ -218,11 +248,27 @@ void Server::fetch(uint64_t id, float* rgb, size_t n, pt_request_stats* st) {
         st->state = r.state;
     }
     if (r.state == PT_REQ_DONE && rgb) {
+        const size_t bytes = 3 * size_t(r.req.width) * size_t(r.req.height) * sizeof(float);
         if (n < 3 * size_t(r.req.width) * size_t(r.req.height)) throw Error{PT_ERR_INVALID, "fetch: buffer too small"};
-        std::memcpy(rgb, r.result, 3 * size_t(r.req.width) * size_t(r.req.height) * sizeof(float));
+        // The copy out of device memory runs outside the lock (the server loop goes on meanwhile); no
+        // other call can release the request while `reading` is set.
+        r.reading = true;
+        g.unlock();
+        try {
+            read_result(r, rgb, 0, bytes);
+        } catch (...) {
+            g.lock();
+            r.reading = false;
+            throw;
+        }
+        g.lock();
+        r.reading = false;
     }
     int state = r.state;
-    pinned_release(r.result, r.result_bytes);
+    if (r.result) {
+        PTW_CUDA(cudaFreeAsync(r.result, fin_stream_));
+        bytes_in_use_ -= r.result_bytes;
+    }
     r.result = nullptr;
     r.fetched = true;
     if (r.batch_refs == 0) requests_.erase(it);  // else the loop erases it after its last batch
@@ -237,25 +283,36 @@ void Server::fetch_encoded(uint64_t id, int format, uint8_t* out, size_t capacit
     if (r.state == PT_REQ_QUEUED || r.state == PT_REQ_RUNNING) throw Error{PT_ERR_INVALID, "request not finished"};
     if (r.state == PT_REQ_CANCELLED) throw Error{PT_ERR_CANCELLED, "request cancelled"};
     if (r.state == PT_REQ_FAILED) throw Error{PT_ERR_CUDA, "request failed: " + r.error};
-    if (r.encoding) throw Error{PT_ERR_INVALID, "fetch: another call is encoding this request"};
+    if (r.reading) throw Error{PT_ERR_INVALID, "fetch: another call is reading this request"};
     if (format == PT_IMAGE_PNG && !r.req.display) throw Error{PT_ERR_INVALID, "PNG: the request was not submitted with display = 1"};
     if (r.encoded_format != format) {
-        // Encoding (PNG: zlib) takes milliseconds: it runs outside the lock. The request cannot go
-        // away meanwhile: only a fetch consumes it, and fetches refuse a request being encoded.
-        r.encoding = true;
-        const float* rgb = r.result;
+        // The copy out and the encoding (PNG: zlib) take milliseconds: they run outside the lock.
+        // The request cannot go away meanwhile: fetches refuse a request that is being read.
+        r.reading = true;
         const int w = r.req.width, h = r.req.height;
+        const size_t npix = size_t(w) * size_t(h);
         lk.unlock();
         std::vector<uint8_t> enc;
         bool ok = true;
         try {
-            if (format == PT_IMAGE_PFM) enc = encode_pfm(rgb, w, h);
-            else ok = encode_png(reinterpret_cast<const uint32_t*>(rgb + 3 * size_t(w) * size_t(h)), w, h, 6, enc);
+            if (format == PT_IMAGE_PFM) {
+                std::vector<float> rgb(3 * npix);
+                read_result(r, rgb.data(), 0, rgb.size() * sizeof(float));
+                enc = encode_pfm(rgb.data(), w, h);
+            } else {
+                std::vector<uint32_t> rgba(npix);
+                read_result(r, rgba.data(), 3 * npix * sizeof(float), npix * sizeof(uint32_t));
+                ok = encode_png(rgba.data(), w, h, 6, enc);
+            }
         } catch (const std::bad_alloc&) {
             ok = false;
+        } catch (...) {
+            lk.lock();
+            r.reading = false;
+            throw;
         }
         lk.lock();
-        r.encoding = false;
+        r.reading = false;
         if (!ok) throw Error{PT_ERR_ALLOC, "fetch: encoding failed"};
         r.encoded = std::move(enc);
         r.encoded_format = format;
@@ -264,11 +321,123 @@ void Server::fetch_encoded(uint64_t id, int format, uint8_t* out, size_t capacit
     if (!out) return;  // a size query keeps the request
     if (capacity < r.encoded.size()) throw Error{PT_ERR_INVALID, "fetch: buffer too small"};
     std::memcpy(out, r.encoded.data(), r.encoded.size());
-    pinned_release(r.result, r.result_bytes);
+    if (r.result) {
+        PTW_CUDA(cudaFreeAsync(r.result, fin_stream_));
+        bytes_in_use_ -= r.result_bytes;
+    }
     r.result = nullptr;
     r.encoded = std::vector<uint8_t>();
     r.fetched = true;
     if (r.batch_refs == 0) requests_.erase(it);  // else the loop erases it after its last batch
+}
+
+int32_t Server::open_session(int32_t scene_id, int w, int h, const pt_svgf_settings& sv) {
+    if (w <= 0 || h <= 0 || uint64_t(w) * uint64_t(h) > (uint64_t(1) << 30))
+        throw Error{PT_ERR_INVALID, "session: width and height must be positive, at most 2^30 pixels"};
+    if (sv.atrous_iterations < 0 || sv.atrous_iterations > 30) throw Error{PT_ERR_INVALID, "session: atrous_iterations out of range"};
+    const size_t npix = size_t(w) * size_t(h);
+    // G-buffer (6), denoised image, and the denoiser's own eight buffers (with tile padding).
+    const size_t estimate = 16 * npix * sizeof(float4) + (size_t(1) << 20);
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        if (scene_id < 0 || scene_id >= int(scenes_.size())) throw Error{PT_ERR_NOT_FOUND, "session: unknown scene"};
+        if (cfg_.budget_bytes && bytes_in_use_ + estimate + pool_bytes_ + scene_bytes_ > cfg_.budget_bytes)
+            throw Error{PT_ERR_BUDGET, "session: does not fit the device-memory budget"};
+    }
+    auto s = std::make_unique<Session>();
+    s->scene = scene_id;
+    s->w = w;
+    s->h = h;
+    s->sv = sv;
+    PTW_CUDA(cudaSetDevice(device_));
+    for (DeviceBuffer<float4>* b : {&s->albedo, &s->normal_depth, &s->emission, &s->color, &s->edge, &s->motion, &s->denoised}) {
+        b->allocate(npix);
+        PTW_CUDA(cudaMemsetAsync(b->ptr, 0, npix * sizeof(float4), fin_stream_));
+    }
+    s->svgf = std::make_unique<SvgfDenoiser>(device_, fin_stream_);
+    s->svgf->resize(w, h);
+    s->bytes = 7 * npix * sizeof(float4) + s->svgf->device_bytes();
+    std::lock_guard<std::mutex> g(mu_);
+    if (cfg_.budget_bytes && bytes_in_use_ + s->bytes + pool_bytes_ + scene_bytes_ > cfg_.budget_bytes)
+        throw Error{PT_ERR_BUDGET, "session: does not fit the device-memory budget"};
+    s->id = next_session_++;
+    bytes_in_use_ += s->bytes;
+    const int32_t id = s->id;
+    sessions_[id] = std::move(s);
+    return id;
+}
+
+// Called with the lock held.
+void Server::free_session_if_closed(Session& s) {
+    if (!s.closed || s.busy) return;
+    bytes_in_use_ -= s.bytes;
+    sessions_.erase(s.id);  // no frame of it is on the device: its buffers are idle
+}
+
+// Called with the lock held, once a session frame has left the device (finished, cancelled, failed).
+void Server::session_frame_ended(Request& r) {
+    if (!r.ses) return;
+    Session* s = r.ses;
+    r.ses = nullptr;
+    s->busy = false;
+    free_session_if_closed(*s);
+    cv_work_.notify_all();  // its next frame may be admitted
+}
+
+void Server::close_session(int32_t session) {
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = sessions_.find(session);
+    if (it == sessions_.end() || it->second->closed) throw Error{PT_ERR_NOT_FOUND, "unknown session"};
+    Session& s = *it->second;
+    s.closed = true;
+    // Frames still waiting for admission end cancelled; a frame on the device finishes first.
+    for (auto q = queue_.begin(); q != queue_.end();) {
+        Request& r = *requests_[*q];
+        if (r.session != session) {
+            ++q;
+            continue;
+        }
+        r.state = PT_REQ_CANCELLED;
+        r.done_s = now();
+        st_.cancelled++;
+        q = queue_.erase(q);
+    }
+    cv_done_.notify_all();
+    free_session_if_closed(s);
+}
+
+uint64_t Server::submit_frame(int32_t session, const pt_camera& cam, const pt_camera& prev, const pt_render_settings& rs) {
+    if (rs.path.max_depth < 0 || rs.path.max_depth > 65535) throw Error{PT_ERR_INVALID, "frame: max_depth must be in [0, 65535]"};
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = sessions_.find(session);
+    if (it == sessions_.end() || it->second->closed) throw Error{PT_ERR_NOT_FOUND, "unknown session"};
+    Session& s = *it->second;
+    auto q = std::make_unique<Request>();
+    q->id = next_id_++;
+    q->req = pt_request{};
+    q->req.scene_id = s.scene;
+    q->req.camera = cam;
+    q->req.width = s.w;
+    q->req.height = s.h;
+    q->req.spp = 1;
+    q->req.seed = rs.seed;
+    q->req.path = rs.path;
+    q->session = session;
+    q->prev = prev;
+    q->frame = s.frames++;
+    q->submit_s = now();
+    q->bytes = request_bytes(q->req);
+    q->work = uint64_t(s.w) * uint64_t(s.h);
+    if (cfg_.budget_bytes && q->bytes + pool_bytes_ + scene_bytes_ > cfg_.budget_bytes) {
+        st_.rejected++;
+        throw Error{PT_ERR_BUDGET, "frame: larger than the device-memory budget"};
+    }
+    const uint64_t id = q->id;
+    requests_[id] = std::move(q);
+    queue_.push_back(id);
+    st_.submitted++;
+    cv_work_.notify_all();
+    return id;
 }
 
 void Server::cancel(uint64_t id) {
@@ -349,44 +518,24 @@ void Server::release_buffers(Request& r, cudaStream_t s) {
     r.sample_out = r.accum = nullptr;
 }
 
-// Pinned host staging for finished images (the result a fetch copies out), reused across requests.
-// Blocks come in power-of-two sizes (at least 64 KiB) and are kept by size; a request takes the
-// smallest one that fits. Pinning is slow, so after a warm-up the pool serves every request.
-static size_t pinned_class(size_t bytes) {
-    size_t c = size_t(1) << 16;
-    while (c < bytes) c <<= 1;
-    return c;
-}
-
-float* Server::pinned_acquire(size_t bytes) {
-    bytes = pinned_class(bytes);
-    {
-        std::lock_guard<std::mutex> g(pinned_mu_);
-        auto it = pinned_free_.lower_bound(bytes);
-        if (it != pinned_free_.end()) {
-            float* p = it->second;
-            pinned_free_.erase(it);
-            return p;
-        }
-    }
-    float* p = nullptr;
-    PTW_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&p), bytes, cudaHostAllocDefault));
-    return p;
-}
-
-void Server::pinned_release(float* p, size_t bytes) {
-    if (!p) return;
-    bytes = pinned_class(bytes);
-    std::lock_guard<std::mutex> g(pinned_mu_);
-    pinned_free_.emplace(bytes, p);
-}
-
 // Called with the lock held: allocates the request's buffers and its finished-path counter. Its work
 // is handed to the wavefront later, chunk by chunk (append_chunks).
-bool Server::try_admit(Request& r) {
-    const int max_active = cfg_.max_active > 0 ? cfg_.max_active : (cfg_.max_active == 0 ? kDefaultMaxActive : 0);
-    if (max_active > 0 && int(active_.size()) >= max_active) return false;
-    if (cfg_.budget_bytes && bytes_in_use_ + r.bytes + pool_bytes_ + scene_bytes_ > cfg_.budget_bytes) return false;
+Server::Admit Server::try_admit(Request& r) {
+    Session* ses = nullptr;
+    if (r.session >= 0) {
+        // Session frames run one at a time per session, and are not held back by the limit on
+        // requests at once (they are small, and latency is their point).
+        auto it = sessions_.find(r.session);
+        if (it == sessions_.end()) return kSkipped;  // (closing a session cancels its queued frames)
+        ses = it->second.get();
+        if (ses->busy) return kSkipped;
+    } else {
+        const int max_active = cfg_.max_active > 0 ? cfg_.max_active : (cfg_.max_active == 0 ? kDefaultMaxActive : 0);
+        int requests = 0;
+        for (uint64_t id : active_) requests += requests_[id]->session < 0 ? 1 : 0;
+        if (max_active > 0 && requests >= max_active) return kBlocked;
+    }
+    if (cfg_.budget_bytes && bytes_in_use_ + r.bytes + pool_bytes_ + scene_bytes_ > cfg_.budget_bytes) return kBlocked;
     size_t npix = size_t(r.req.width) * size_t(r.req.height);
     try {
         if (inject_failures_ > 0) {
@@ -404,7 +553,7 @@ bool Server::try_admit(Request& r) {
         r.error = e.message;
         r.done_s = now();
         cv_done_.notify_all();
-        return true;  // consumed (failed), not retried
+        return kAdmitted;  // consumed (failed), not retried
     }
     // Grow the finished-path counters by doubling.
     if (size_t(done_slots_) + 1 > d_done_.count) {
@@ -438,12 +587,30 @@ bool Server::try_admit(Request& r) {
     v.clamp = r.req.path.clamp;
     v.sample_out = r.sample_out;
     v.accum = r.accum;
+    if (ses) {
+        // The frame's first vertex writes the session's G-buffer and the denoiser's records, as
+        // pt_render_denoised's frame does; its sample index is the frame number.
+        v.frame0 = r.frame;
+        v.gbuffer = 1;
+        v.realtime = 1;
+        v.g_albedo = ses->albedo.ptr;
+        v.g_normal_depth = ses->normal_depth.ptr;
+        v.g_emission = ses->emission.ptr;
+        v.g_color = ses->color.ptr;
+        v.g_edge = ses->edge.ptr;
+        v.g_motion = ses->motion.ptr;
+        static_assert(sizeof(v.prev_cam) == sizeof(pt_camera), "camera layout");
+        std::memcpy(v.prev_cam, &r.prev, sizeof(v.prev_cam));
+        v.has_prev = 1;
+        ses->busy = true;
+        r.ses = ses;
+    }
     v.done_counter = d_done_.ptr + r.done_slot;
     bytes_in_use_ += r.bytes;
     r.state = PT_REQ_RUNNING;
     r.admit_s = now();
     active_.push_back(r.id);
-    return true;
+    return kAdmitted;
 }
 
 // Called with the lock held: hands chunks of the running requests' work to the wavefront, shortest
@@ -488,10 +655,25 @@ void Server::loop() {
         std::vector<Request*> done;      // requests whose image has landed in host memory this turn
         try {
             // Admission in arrival order while the budget allows, then chunks of work.
-            while (!queue_.empty()) {
-                Request& r = *requests_[queue_.front()];
-                if (!try_admit(r)) break;
-                queue_.pop_front();
+            // Admission in arrival order: a request that does not fit holds back the requests behind
+            // it, but not session frames (which wait only for their own session's previous frame).
+            bool held = false;
+            for (auto q = queue_.begin(); q != queue_.end();) {
+                Request& r = *requests_[*q];
+                if (held && r.session < 0) {
+                    ++q;
+                    continue;
+                }
+                const Admit a = try_admit(r);
+                if (a == kAdmitted) {
+                    q = queue_.erase(q);
+                    continue;
+                }
+                if (a == kBlocked) {
+                    if (r.session >= 0) break;  // the budget: nothing behind it fits either
+                    held = true;
+                }
+                ++q;
             }
             append_chunks();
             if (scenes_dirty_) upload_scene_table();
@@ -502,8 +684,20 @@ void Server::loop() {
             Batch& B = batch_[cur];
             Batch& P = batch_[cur ^ 1];
             if (views_uploaded_ < views_.size()) {
-                PTW_CUDA(cudaMemcpyAsync(d_views_.ptr + views_uploaded_, views_.data() + views_uploaded_,
-                                         (views_.size() - views_uploaded_) * sizeof(DevView), cudaMemcpyHostToDevice, stream_));
+                // New view-table entries go up through B's pinned staging (B's previous batch has
+                // completed): a copy from pageable memory could hold this thread until the stream
+                // drains, and the device would idle while the host turns around.
+                const size_t n_new = views_.size() - views_uploaded_;
+                if (n_new > B.views_cap) {
+                    if (B.views) PTW_CUDA(cudaFreeHost(B.views));
+                    B.views = nullptr;
+                    B.views_cap = 0;
+                    const size_t cap = std::max<size_t>(2 * n_new, 4096);
+                    PTW_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&B.views), cap * sizeof(DevView), cudaHostAllocDefault));
+                    B.views_cap = cap;
+                }
+                std::memcpy(B.views, views_.data() + views_uploaded_, n_new * sizeof(DevView));
+                PTW_CUDA(cudaMemcpyAsync(d_views_.ptr + views_uploaded_, B.views, n_new * sizeof(DevView), cudaMemcpyHostToDevice, stream_));
                 views_uploaded_ = views_.size();
                 if (!engine_started_) {
                     engine_->begin(d_scenes_.ptr, d_views_.ptr, int(views_.size()));
@@ -570,6 +764,7 @@ void Server::loop() {
                 engine_->set_continuous_sorting(pending >= kSortMinPaths);
                 PTW_CUDA(cudaEventRecord(B.ev_start, stream_));
                 engine_->launch(B.iterations);
+                batches_++;
                 PTW_CUDA(cudaMemcpyAsync(B.ctr, engine_->device_counters(), sizeof(Counters), cudaMemcpyDeviceToHost, stream_));
                 if (B.n)
                     PTW_CUDA(cudaMemcpyAsync(B.done, d_done + B.lo, B.n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_));
@@ -588,6 +783,7 @@ void Server::loop() {
                 // arrivals are seen soon.
                 float ms = 0.0f;
                 if (cudaEventElapsedTime(&ms, P.ev_start, P.ev) == cudaSuccess && ms > 0.0f) {
+                    device_ms_ += ms;
                     double want = double(P.iterations) * (1.0 / double(ms));
                     iters_per_batch_ = std::max(1, std::min(16, int(want + 0.5)));
                 }
@@ -597,21 +793,32 @@ void Server::loop() {
                     r->finishing = true;  // the batch launched meanwhile also lists it: finish once
                     (r->cancel ? cancelled : finished).push_back(r);
                 }
-                // Sum each finished request's samples in order and copy its image out, on the second
-                // stream after the batch that finished it; release its buffers behind the copy.
+                // Sum each finished request's samples in order and resolve its image into a device
+                // result buffer that fetch copies out, on the second stream after the batch that
+                // finished it; release its sample buffers behind it. (Results stay on the device: an
+                // allocation of pinned host memory here would stall this thread and idle the device.)
                 for (Request* r : finished) {
                     const uint32_t npix = uint32_t(r->req.width) * uint32_t(r->req.height);
                     const int first = r->views.front();  // carries the whole image's spp and buffers
                     PTW_CUDA(cudaStreamWaitEvent(fin_stream_, P.ev, 0));
                     PTW_CUDA(wf_accumulate(d_views_.ptr + first, views_[size_t(first)], 1, 1, fin_stream_));
-                    // The averaged rgb image goes into the (no longer needed) sample buffer, then to
-                    // pinned host memory that fetch copies from.
-                    float* rgb = reinterpret_cast<float*>(r->sample_out);
-                    PTW_CUDA(wf_resolve(r->accum, npix, 1.0f / float(r->req.spp), true, rgb, fin_stream_));
-                    r->result_bytes = size_t(npix) * 3 * sizeof(float);
+                    r->result_bytes = size_t(npix) * (3 * sizeof(float) + (r->req.display ? sizeof(uint32_t) : 0));
+                    PTW_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->result), r->result_bytes, mem_pool_, fin_stream_));
+                    float* rgb = r->result;
+                    if (r->ses) {
+                        // A session frame: the accumulate step above wrote its colour; denoise it with
+                        // the session's history (on this stream, in the session's frame order) and
+                        // hand out the denoised image.
+                        Session& ses = *r->ses;
+                        ses.svgf->run_frame(reinterpret_cast<const float*>(ses.color.ptr), reinterpret_cast<const float*>(ses.albedo.ptr),
+                                            reinterpret_cast<const float*>(ses.emission.ptr), reinterpret_cast<const float*>(ses.edge.ptr),
+                                            reinterpret_cast<const float*>(ses.motion.ptr), ses.sv, reinterpret_cast<float*>(ses.denoised.ptr));
+                        PTW_CUDA(wf_resolve(ses.denoised.ptr, npix, 1.0f, false, rgb, fin_stream_));
+                    } else {
+                        PTW_CUDA(wf_resolve(r->accum, npix, 1.0f / float(r->req.spp), true, rgb, fin_stream_));
+                    }
                     if (r->req.display) {
-                        // The colour view of pt_display on the summed samples, into the rest of the
-                        // sample buffer (it holds spp >= 1 float4 per pixel: room for 12 + 4 bytes).
+                        // The colour view of pt_display on the summed samples, after the float image.
                         DisplayParams dp{};
                         dp.w = r->req.width;
                         dp.h = r->req.height;
@@ -624,10 +831,7 @@ void Server::loop() {
                         dp.heat_scale = 1.0f / 160.0f;
                         uint32_t* rgba = reinterpret_cast<uint32_t*>(rgb + 3 * size_t(npix));
                         PTW_CUDA(wf_display(dp, r->accum, nullptr, nullptr, nullptr, nullptr, nullptr, rgba, fin_stream_));
-                        r->result_bytes += size_t(npix) * sizeof(uint32_t);
                     }
-                    r->result = pinned_acquire(r->result_bytes);
-                    PTW_CUDA(cudaMemcpyAsync(r->result, rgb, r->result_bytes, cudaMemcpyDeviceToHost, fin_stream_));
                     release_buffers(*r, fin_stream_);
                     Finishing f{r, nullptr};
                     PTW_CUDA(cudaEventCreateWithFlags(&f.ev, cudaEventDisableTiming));
@@ -657,6 +861,8 @@ void Server::loop() {
             }
             lk.lock();
             st_.bounce_iterations = iterations_;
+            st_.device_seconds = device_ms_ / 1000.0;
+            st_.batches = batches_;
             // A request leaves the active list once its image is being finished (the next batches no
             // longer carry it); its memory counts against the budget until the copy has landed.
             auto deactivate = [&](Request* r) { active_.erase(std::remove(active_.begin(), active_.end(), r->id), active_.end()); };
@@ -667,13 +873,16 @@ void Server::loop() {
                 r->done_s = now();
                 bytes_in_use_ -= r->bytes;
                 st_.cancelled++;
+                session_frame_ended(*r);
             }
             for (Request* r : done) {
                 r->state = PT_REQ_DONE;
                 r->done_s = now();
                 bytes_in_use_ -= r->bytes;
+                bytes_in_use_ += r->result_bytes;  // its result, until fetched
                 st_.completed++;
                 st_.samples_done += r->work;
+                session_frame_ended(*r);
             }
             if (!done.empty() || !cancelled.empty()) cv_done_.notify_all();
             release_batch_refs(released);
@@ -695,11 +904,13 @@ void Server::loop() {
             // and one whose copy landed in this turn has already left finishing_ for `done`.
             for (Request* r : done) {
                 if (r->state != PT_REQ_RUNNING) continue;
-                r->state = PT_REQ_DONE;  // its image is in host memory
+                r->state = PT_REQ_DONE;  // its image is complete
                 r->done_s = now();
                 bytes_in_use_ -= r->bytes;
+                bytes_in_use_ += r->result_bytes;
                 st_.completed++;
                 st_.samples_done += r->work;
+                session_frame_ended(*r);
             }
             for (Finishing& f : finishing_) {
                 cudaEventDestroy(f.ev);
@@ -708,6 +919,9 @@ void Server::loop() {
                 f.r->error = e.message;
                 f.r->done_s = now();
                 bytes_in_use_ -= f.r->bytes;
+                if (f.r->result) cudaFreeAsync(f.r->result, fin_stream_);
+                f.r->result = nullptr;
+                session_frame_ended(*f.r);
             }
             finishing_.clear();
             // A device failure fails every running request; the server keeps its handle valid.
@@ -717,11 +931,14 @@ void Server::loop() {
                     release_buffers(r, stream_);
                     continue;
                 }
+                session_frame_ended(r);
                 r.state = PT_REQ_FAILED;
                 r.error = e.message;
                 r.done_s = now();
                 bytes_in_use_ -= r.bytes;
                 release_buffers(r, stream_);
+                if (r.result) cudaFreeAsync(r.result, fin_stream_);  // allocated before the failure
+                r.result = nullptr;
             }
             active_.clear();
             cv_done_.notify_all();

@@ -13,6 +13,7 @@
 
 #include "photon_wavefront.h"
 #include "renderer.h"
+#include "svgf.h"
 
 namespace ptw {
 
@@ -38,7 +39,26 @@ public:
     // A tuning record (pt_server_set_tuning): its scheduling knobs apply from the next batch.
     void set_tuning(const pt_tuning& t);
 
+    // Real-time SVGF sessions served beside the requests (pt_server_open_session and friends).
+    int32_t open_session(int32_t scene_id, int w, int h, const pt_svgf_settings& sv);
+    void close_session(int32_t session);
+    uint64_t submit_frame(int32_t session, const pt_camera& cam, const pt_camera& prev, const pt_render_settings& rs);
+
 private:
+    // A session: the G-buffer of its frames and its denoiser history, on the server's device. Its
+    // frames are requests of one path per pixel whose first vertex writes the G-buffer and whose
+    // finishing step denoises it; one frame is on the device at a time, in submission order.
+    struct Session {
+        int id = 0, scene = 0, w = 0, h = 0;
+        pt_svgf_settings sv{};
+        std::unique_ptr<SvgfDenoiser> svgf;  // on the finishing stream
+        DeviceBuffer<float4> albedo, normal_depth, emission, color, edge, motion, denoised;
+        uint32_t frames = 0;  // frames submitted: the next frame's sample index
+        bool busy = false;    // a frame is admitted and not finished
+        bool closed = false;
+        size_t bytes = 0;
+    };
+
     struct Request {
         uint64_t id;
         pt_request req;
@@ -59,22 +79,29 @@ private:
         std::string error;
         float4* sample_out = nullptr;  // stream-ordered allocations from the server's memory pool
         float4* accum = nullptr;
-        float* result = nullptr;  // rgb (pinned, from the server's staging pool), filled when done; with
-                                  // req.display the RGBA8 display image follows the 3 * pixels floats
+        int session = -1;         // a session frame: its session id, previous camera and sample index
+        pt_camera prev{};
+        uint32_t frame = 0;
+        Session* ses = nullptr;   // set at admission (the session lives while a frame of it runs)
+        float* result = nullptr;  // the finished image on the device (from the request pool): rgb floats,
+                                  // and with req.display the RGBA8 display image after them; held until
+                                  // fetched (counted against the budget meanwhile)
         size_t result_bytes = 0;
         std::vector<uint8_t> encoded;  // the image in encoded_format, kept by a size query
         int encoded_format = -1;
-        bool encoding = false;         // a fetch_encoded call is encoding it outside the lock
+        bool reading = false;          // a fetch is copying its result out, outside the lock
     };
 
     void loop();
     double now() const;
     size_t request_bytes(const pt_request& r) const;
-    bool try_admit(Request& r);
+    enum Admit { kAdmitted, kBlocked, kSkipped };
+    Admit try_admit(Request& r);
+    void session_frame_ended(Request& r);  // with the lock held: the session may take its next frame
+    void free_session_if_closed(Session& s);
     void append_chunks();
     void release_buffers(Request& r, cudaStream_t s);
-    float* pinned_acquire(size_t bytes);
-    void pinned_release(float* p, size_t bytes);
+    void read_result(const Request& r, void* dst, size_t offset, size_t bytes);  // device -> caller memory
     void upload_scene_table();
     void release_batch_refs(const std::vector<Request*>& reqs);
 
@@ -94,6 +121,8 @@ private:
     size_t scene_bytes_ = 0;
 
     std::map<uint64_t, std::unique_ptr<Request>> requests_;
+    std::map<int32_t, std::unique_ptr<Session>> sessions_;
+    int32_t next_session_ = 1;
     std::deque<uint64_t> queue_;
     std::vector<uint64_t> active_;
     uint64_t next_id_ = 1;
@@ -113,6 +142,8 @@ private:
         unsigned long long* done = nullptr;      // pinned, finished-path counters [lo, lo + n)
         size_t done_cap = 0, lo = 0, n = 0;
         unsigned long long* work_total = nullptr;  // pinned staging of the work total
+        DevView* views = nullptr;                // pinned staging of the view-table entries it uploads
+        size_t views_cap = 0;
         std::vector<Request*> reqs;              // active requests when the batch was launched
         std::vector<uint64_t> need;              // their paths to finish (all, or those handed over if cancelled)
         cudaEvent_t ev = nullptr, ev_start = nullptr;
@@ -122,16 +153,16 @@ private:
     Batch batch_[2];
     struct Finishing {
         Request* r;
-        cudaEvent_t ev;  // its image has landed in r->result
+        cudaEvent_t ev;  // its image is complete in r->result
     };
     std::vector<Finishing> finishing_;
-    std::mutex pinned_mu_;
-    std::multimap<size_t, float*> pinned_free_;
     int iters_per_batch_ = 2;  // adapted so that a batch keeps the device busy for about a millisecond
     cudaStream_t fin_stream_ = nullptr;
     uint64_t generated_ = 0;       // work items generated, as of the last completed batch
     uint64_t queued_ = 0;          // paths queued for the next iteration, as of the last completed batch
     uint64_t iterations_ = 0;
+    double device_ms_ = 0;         // device time of completed batches
+    uint64_t batches_ = 0;
     size_t views_uploaded_ = 0;
     uint64_t work_total_ = 0;
     size_t bytes_in_use_ = 0;

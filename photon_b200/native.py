@@ -63,6 +63,10 @@ def _load():
         "pt_autotune_views": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_uint64, P(abi.Tuning), P(C.c_double), P(C.c_double)],
                               C.c_int32),
         "pt_server_set_tuning": ([C.c_void_p, P(abi.Tuning)], C.c_int32),
+        "pt_server_open_session": ([C.c_void_p, C.c_int32, C.c_int32, C.c_int32, P(abi.SvgfSettings), P(C.c_int32)], C.c_int32),
+        "pt_server_submit_frame": ([C.c_void_p, C.c_int32, P(abi.Camera), P(abi.Camera), P(abi.RenderSettings), P(C.c_uint64)],
+                                   C.c_int32),
+        "pt_server_close_session": ([C.c_void_p, C.c_int32], C.c_int32),
         "pt_server_fetch_encoded": ([C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p, C.c_size_t, P(C.c_size_t)], C.c_int32),
         "pt_trace_primary": ([C.c_void_p, P(abi.Camera), C.c_int32, C.c_int32, C.c_uint32, C.c_uint32, _f32p], C.c_int32),
         "pt_light_picks_primary": ([C.c_void_p, P(abi.Camera), P(abi.RenderSettings), C.c_uint32, _i32p], C.c_int32),
@@ -369,8 +373,8 @@ def encode_png(rgba, level=6):
 class Server:
     """The request server (continuous batching over resident scenes)."""
 
-    def __init__(self, budget_bytes=0, device=0, path_capacity=0, max_active=0, device_wait_seconds=2.0, sort_rays=0):
-        cfg = abi.ServerConfig(device, budget_bytes, path_capacity, max_active, device_wait_seconds, sort_rays)
+    def __init__(self, budget_bytes=0, device=0, path_capacity=0, max_active=0, device_wait_seconds=2.0, sort_rays=0, reserve_bytes=0):
+        cfg = abi.ServerConfig(device, budget_bytes, path_capacity, max_active, device_wait_seconds, sort_rays, reserve_bytes)
         p = C.c_void_p()
         _check(lib.pt_server_create(C.byref(cfg), C.byref(p)), lib.pt_global_error)
         self.h = p
@@ -406,6 +410,22 @@ class Server:
 
     def cancel(self, rid):
         _check(lib.pt_server_cancel(self.h, rid), self._err)
+
+    def open_session(self, scene_id, w, h, svgf=None):
+        """A real-time SVGF session on a resident scene (pt_server_open_session); returns its id."""
+        sid = C.c_int32()
+        _check(lib.pt_server_open_session(self.h, scene_id, w, h, C.byref(svgf or abi.svgf_settings()), C.byref(sid)), self._err)
+        return sid.value
+
+    def submit_frame(self, session, cam, prev, rs):
+        """One frame of a session (1 spp + G-buffer + SVGF with the session's history); returns a
+        request id for wait / poll / fetch."""
+        rid = C.c_uint64()
+        _check(lib.pt_server_submit_frame(self.h, session, C.byref(cam), C.byref(prev), C.byref(rs), C.byref(rid)), self._err)
+        return rid.value
+
+    def close_session(self, session):
+        _check(lib.pt_server_close_session(self.h, session), self._err)
 
     def encoded_size(self, rid, fmt):
         """Size of the request's image in `fmt` (abi.PT_IMAGE_*); the request stays."""

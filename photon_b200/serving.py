@@ -16,7 +16,10 @@ def _summary(lat, samples, makespan):
 
 
 def run_served(server, stream, timeout_s=600.0):
-    """Submits each request at its arrival time; latency = server-side done time - submit time."""
+    """Submits each request at its arrival time; latency = server-side done time - submit time. Also
+    reports the device time of the server's bounce-iteration batches over the run (busy fraction of its
+    stream) and the batches and iterations it launched."""
+    st0 = server.stats()
     ids = [None] * len(stream)
     t0 = time.perf_counter()
 
@@ -40,7 +43,59 @@ def run_served(server, stream, timeout_s=600.0):
         first = st.submit_s if first is None else min(first, st.submit_s)
         last = st.done_s if last is None else max(last, st.done_s)
     th.join()
-    return _summary(lat, samples, last - first)
+    st1 = server.stats()
+    out = _summary(lat, samples, last - first)
+    out.update(device_busy=(st1.device_seconds - st0.device_seconds) / max(last - first, 1e-9), batches=st1.batches - st0.batches,
+               iterations=st1.bounce_iterations - st0.bounce_iterations)
+    return out
+
+
+def run_sessions_served(server, scene_id, desc, n_sessions=8, frames=120, width=1600, height=900, max_depth=12, warmup=3,
+                        stream=None):
+    """Real-time SVGF sessions as a request class of `server` (pt_server_open_session): each session,
+    on its own host thread, submits the frames of an orbit of the scene one after the other (frame
+    k + 1 once frame k has been fetched). With `stream`, that request stream is served at the same time
+    (run_served) and its summary returned beside the sessions'. Frame latency = server-side done time -
+    submit time."""
+    from . import workloads
+    rs = abi.render_settings(width, height, max_depth=max_depth, seed=11)
+    sv = abi.svgf_settings()
+    sessions = [server.open_session(scene_id, width, height, sv) for _ in range(n_sessions)]
+    cams = [workloads.orbit_cameras(desc, frames + warmup, width / height, start_deg=45.0 * k) for k in range(n_sessions)]
+    lat = [[] for _ in range(n_sessions)]
+    barrier = threading.Barrier(n_sessions + 1)
+
+    def frame(k, f):
+        rid = server.submit_frame(sessions[k], cams[k][f], cams[k][max(f - 1, 0)], rs)
+        server.wait(rid, 600.0)
+        _, st = server.fetch(rid, width, height)
+        return st.done_s - st.submit_s
+
+    def session(k):
+        for f in range(warmup):
+            frame(k, f)
+        barrier.wait()
+        for f in range(warmup, warmup + frames):
+            lat[k].append(frame(k, f))
+
+    threads = [threading.Thread(target=session, args=(k,)) for k in range(n_sessions)]
+    for t in threads:
+        t.start()
+    barrier.wait()
+    t0 = time.perf_counter()
+    served = run_served(server, stream) if stream else None
+    for t in threads:
+        t.join()
+    wall = time.perf_counter() - t0
+    for sid in sessions:
+        server.close_session(sid)
+    ms = np.asarray([t for ts in lat for t in ts]) * 1e3
+    out = {"sessions": n_sessions, "frames": int(ms.size), "width": width, "height": height, "spp": 1,
+           "p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)), "mean_ms": float(ms.mean()),
+           "frames_per_s": ms.size / wall, "msamples_per_s": ms.size * width * height / wall / 1e6}
+    if served is not None:
+        out["stream"] = served
+    return out
 
 
 def run_plain(renderers, stream):

@@ -377,3 +377,73 @@ def test_server_serves_encoded_images(server_scenes):
     assert np.array_equal(img.view(np.uint32), img_c.view(np.uint32))
     assert pfm == native.encode_pfm(img)
     assert np.array_equal(png, disp)
+
+
+def test_server_sessions_equal_render_denoised_alone_and_under_load(server_scenes):
+    """Real-time SVGF sessions served as a request class: each frame (one path per pixel, G-buffer,
+    SVGF with the session's history) fetched from the server equals the same frame sequence through a
+    renderer's pt_render_denoised, bit for bit. This holds for a session alone, and for frames
+    submitted all at once (they run one at a time, in order) while ordinary requests flood the server
+    and share its path pool. Closing a session cancels its waiting frames, and the server's memory in
+    use returns to idle."""
+    from photon_b200 import workloads
+    _, (tdesc, tcam, tkeep) = server_scenes
+    w, h, frames = 128, 72, 4
+    cams = workloads.orbit_cameras(tdesc, frames, w / h)
+    prev = [cams[max(f - 1, 0)] for f in range(frames)]
+    rs = abi.render_settings(w, h, max_depth=12, seed=11)
+    sv = abi.svgf_settings()
+    r = native.Renderer()
+    r.upload(tdesc)
+    r.resize(w, h)
+    want = []
+    for f in range(frames):
+        r.render_denoised(cams[f], prev[f], rs, sv)
+        want.append(r.download_image())
+    r.close()
+    s = native.Server(budget_bytes=8 << 30, path_capacity=1 << 18, max_active=2)
+    scene = s.add_scene(tdesc)
+    idle = s.stats().device_bytes_in_use
+    ses = s.open_session(scene, w, h, sv)
+    assert s.stats().device_bytes_in_use > idle
+    for f in range(frames):
+        rid = s.submit_frame(ses, cams[f], prev[f], rs)
+        s.wait(rid, 60)
+        img, st = s.fetch(rid, w, h)
+        assert st.state == abi.PT_REQ_DONE
+        assert np.array_equal(img.view(np.uint32), want[f].view(np.uint32)), f"frame {f} alone"
+    s.close_session(ses)
+    ses = s.open_session(scene, w, h, sv)
+    load = [s.submit(scene, tcam(1.0), 192, 108, 8, seed=100 + k, path=abi.path_options(max_depth=12)) for k in range(10)]
+    rids = [s.submit_frame(ses, cams[f], prev[f], rs) for f in range(frames)]
+    for f, rid in enumerate(rids):
+        s.wait(rid, 120)
+        img, _ = s.fetch(rid, w, h)
+        assert np.array_equal(img.view(np.uint32), want[f].view(np.uint32)), f"frame {f} under load"
+    for rid in load:
+        s.wait(rid, 120)
+        s.fetch(rid, 192, 108)
+    s.close_session(ses)
+    ses = s.open_session(scene, w, h, sv)
+    queued = [s.submit_frame(ses, cams[f], prev[f], rs) for f in range(frames)]
+    s.close_session(ses)
+    states = []
+    for rid in queued:
+        try:
+            s.wait(rid, 60)
+        except native.PhotonError as e:
+            assert e.code == abi.PT_ERR_CANCELLED
+        states.append(s.poll(rid))
+        try:
+            s.fetch(rid, w, h)
+        except native.PhotonError:
+            pass
+    assert states[-1] == abi.PT_REQ_CANCELLED and set(states) <= {abi.PT_REQ_DONE, abi.PT_REQ_CANCELLED}
+    with pytest.raises(native.PhotonError) as e:
+        s.submit_frame(ses, cams[0], prev[0], rs)
+    assert e.value.code == abi.PT_ERR_NOT_FOUND
+    deadline = time.time() + 30
+    while s.stats().device_bytes_in_use != idle and time.time() < deadline:
+        time.sleep(0.05)
+    assert s.stats().device_bytes_in_use == idle
+    s.close()
