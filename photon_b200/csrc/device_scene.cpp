@@ -76,7 +76,7 @@ void validate_scene(const pt_scene_desc& d, bool lights_only) {
 
 size_t DeviceScene::estimate_bytes(const pt_scene_desc& d) {
     size_t b = 0;
-    b += size_t(d.num_nodes) * 64 + size_t(d.num_tris) * (48 + 16);
+    b += size_t(d.num_nodes) * 64 + size_t(d.num_tris) * (16 * kTriStride + 16);
     b += size_t(d.num_vertices) * ((d.normals ? 16 : 0) + (d.uvs ? 8 : 0) + (d.tangents ? 16 : 0));
     b += size_t(d.num_materials) * 80 + size_t(d.num_textures) * 16 + size_t(d.num_texels) * 4 + 1024;
     b += size_t(d.num_emissive) * 24 + size_t(d.num_punctual) * 48;
@@ -152,7 +152,15 @@ void DeviceScene::upload(const pt_scene_desc& d, cudaStream_t s, bool lights_onl
     }
     // What update_lights re-uploads (gpu_renderer.cu:303-310): triangles, materials, light tables
     // and the environment.
-    tris_.upload(reinterpret_cast<const float4*>(d.tris), size_t(d.num_tris) * 3, s);
+    {
+        // Photon's 48-byte TriGeom records, each padded to 64 bytes (kTriStride float4).
+        std::vector<float4> padded(size_t(d.num_tris) * kTriStride, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+        const float4* src = reinterpret_cast<const float4*>(d.tris);
+        for (size_t t = 0; t < size_t(d.num_tris); t++)
+            for (int k = 0; k < 3; k++) padded[t * kTriStride + size_t(k)] = src[t * 3 + size_t(k)];
+        tris_.upload(padded.data(), padded.size(), s);
+        PTW_CUDA(cudaStreamSynchronize(s));
+    }
     materials_.upload(reinterpret_cast<const float4*>(d.materials), size_t(d.num_materials) * 5, s);
     num_materials_ = d.num_materials;
     upload_shade_keys(d.materials, d.num_materials, s);

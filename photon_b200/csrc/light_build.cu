@@ -65,7 +65,7 @@ __global__ void k_light_tris(const float4* __restrict__ materials, float4* __res
                              float* __restrict__ power_out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    float4* g = tris + 3 * size_t(i);
+    float4* g = tris + kTriStride * size_t(i);
     const int mi = __float_as_int(g[0].w);
     const float4* m = materials + 5 * size_t(mi);
     const float4 m1 = m[1], m3 = m[3], m4 = m[4];

@@ -364,7 +364,7 @@ PT_HD V3 emitted(const DevScene& s, int tri, int material, float u, float v) {
     }
     return e;
 }
-PT_HD int tri_material(const DevScene& s, int tri) { return __float_as_int(__ldg(s.tris + 3 * tri).w); }
+PT_HD int tri_material(const DevScene& s, int tri) { return __float_as_int(__ldg(s.tris + kTriStride * tri).w); }
 PT_HD bool mat_double_sided(const DevScene& s, int material) { return __float_as_int(__ldg(s.materials + 5 * material + 3).z) != 0; }
 
 PT_HD float emissive_pdf(const DevScene& s, int tri, int emissive_entry, V3 dir, float dist) {
@@ -372,7 +372,7 @@ PT_HD float emissive_pdf(const DevScene& s, int tri, int emissive_entry, V3 dir,
     int k = emissive_entry;
     if (k < 0) return 0;
     int2 e = __ldg(s.emissive + k);
-    V3 e1 = load_v3(s.tris + 3 * tri + 1), e2 = load_v3(s.tris + 3 * tri + 2);
+    V3 e1 = load_v3(s.tris + kTriStride * tri + 1), e2 = load_v3(s.tris + kTriStride * tri + 2);
     V3 n = normalize(cross(e1, e2));
     float cos_l = fabsf(dot(n, dir));
     if (cos_l <= 0) return 0;
@@ -400,7 +400,7 @@ PT_HD LightSample sample_light(const DevScene& s, V3 p, float u_group, V2 u, flo
             pick->bin = bin >= s.num_emissive ? s.num_emissive - 1 : bin;
         }
         int2 e = __ldg(s.emissive + k);
-        const float4* g = s.tris + 3 * e.x;
+        const float4* g = s.tris + kTriStride * e.x;
         float4 g0 = __ldg(g);
         V3 v0 = xyz(g0), e1 = load_v3(g + 1), e2 = load_v3(g + 2);
         V2 b = uniform_triangle(u);
@@ -491,7 +491,7 @@ PT_HD V3 load_normal(const DevScene& s, int v) { return load_v3(s.normals + v); 
 
 PT_HD Interaction surface_at(const DevScene& s, V3 ro, V3 rd, float t, int tri, float hu, float hv) {
     Interaction it;
-    const float4* g = s.tris + 3 * tri;
+    const float4* g = s.tris + kTriStride * tri;
     float4 g0 = __ldg(g);
     V3 e1 = load_v3(g + 1), e2 = load_v3(g + 2);
     int material = __float_as_int(g0.w);

@@ -85,8 +85,29 @@ PT_HD f32x2 mul2(f32x2 a, f32x2 b) {
     return r;
 }
 
-// The slab test of box_entry with the (bmin - o) * inv_d products computed in pairs; the min/max
-// reduction is unchanged (there is no packed min/max).
+// Three-input min / max (sm_100): one instruction for two of the slab test's reductions. min and max
+// are exact and order-free (a NaN operand is ignored, as fminf / fmaxf ignore it), so the results are
+// those of the two-input chains.
+PT_HD float fmin3(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+PT_HD float fmax3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// 32 bytes (two float4) in one 256-bit load through the read-only path (sm_100); p is 32-byte aligned.
+PT_HD void ldg_pair(const float4* p, float4& a, float4& b) {
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(p));
+}
+
+// The slab test of box_entry with the (bmin - o) * inv_d products computed in pairs and the min/max
+// reductions with three inputs where two chained ones stood.
 struct RayPairs {
     f32x2 oxy, oz0, ixy, iz0;
 };
@@ -97,8 +118,8 @@ PT_HD float box_entry2(float4 bmin, float4 bmax, const RayPairs& r, float tmax) 
     unpack2(mul2(sub2(pack2(bmin.z, bmin.w), r.oz0), r.iz0), tz0, w0);
     unpack2(mul2(sub2(pack2(bmax.x, bmax.y), r.oxy), r.ixy), tx1, ty1);
     unpack2(mul2(sub2(pack2(bmax.z, bmax.w), r.oz0), r.iz0), tz1, w1);
-    float tnear = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
-    float tfar = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
+    float tnear = fmax3(fminf(tx0, tx1), fminf(ty0, ty1), fmaxf(fminf(tz0, tz1), 0.0f));
+    float tfar = fmin3(fmaxf(tx0, tx1), fmaxf(ty0, ty1), fminf(fmaxf(tz0, tz1), tmax));
     return tnear <= tfar ? tnear : kInf;
 }
 
@@ -145,8 +166,10 @@ struct Walker {
     PT_HD bool step(const WalkScene& ws, int* stack, int stride, int* overflow, TraversalCounters* cnt) {
         bool decide = false;
         if (!leaf_mode) {
-            const float4* n = ws.nodes + 4 * node;
-            float4 n0 = __ldg(n), n1 = __ldg(n + 1), n2 = __ldg(n + 2), n3 = __ldg(n + 3);
+            const float4* n = ws.nodes + 4 * node;  // 64-byte nodes: two 256-bit loads
+            float4 n0, n1, n2, n3;
+            ldg_pair(n, n0, n1);
+            ldg_pair(n + 2, n2, n3);
             if (Count) cnt->nodes++;
             float tl = Packed ? box_entry2(n0, n1, rp, tmax) : box_entry(n0, n1, o, inv_d, tmax);
             float tr = Packed ? box_entry2(n2, n3, rp, tmax) : box_entry(n2, n3, o, inv_d, tmax);
@@ -180,8 +203,10 @@ struct Walker {
         }
         if (leaf_mode) {
             int i = ti;
-            const float4* g = ws.tris + 3 * i;
-            float4 g0 = __ldg(g), g1 = __ldg(g + 1), g2 = __ldg(g + 2);
+            const float4* g = ws.tris + kTriStride * i;  // 64-byte records: two 256-bit loads
+            float4 g0, g1, g2, g3;
+            ldg_pair(g, g0, g1);
+            ldg_pair(g + 2, g2, g3);
             float t, tu, tv;
             if (Count) cnt->tris++;
             if (tri_intersect(g0, g1, g2, o, d, tmax, t, tu, tv) &&
@@ -301,9 +326,14 @@ struct AnyWalker4 {
     // ws.nodes: the 4-wide BVH (8 float4 per node).
     PT_HD bool step(const WalkScene& ws, int* stack, int stride, int* overflow, TraversalCounters* cnt) {
         if (!leaf_mode) {
-            const float4* n = ws.nodes + 8 * node;
-            const float4 lx = __ldg(n), ly = __ldg(n + 1), lz = __ldg(n + 2), hx = __ldg(n + 3), hy = __ldg(n + 4), hz = __ldg(n + 5);
-            const int4 id = __ldg(reinterpret_cast<const int4*>(n + 6)), ct = __ldg(reinterpret_cast<const int4*>(n + 7));
+            const float4* n = ws.nodes + 8 * node;  // 128-byte nodes: four 256-bit loads
+            float4 lx, ly, lz, hx, hy, hz, id4, ct4;
+            ldg_pair(n, lx, ly);
+            ldg_pair(n + 2, lz, hx);
+            ldg_pair(n + 4, hy, hz);
+            ldg_pair(n + 6, id4, ct4);
+            const int4 id = make_int4(__float_as_int(id4.x), __float_as_int(id4.y), __float_as_int(id4.z), __float_as_int(id4.w));
+            const int4 ct = make_int4(__float_as_int(ct4.x), __float_as_int(ct4.y), __float_as_int(ct4.z), __float_as_int(ct4.w));
             if (Count) cnt->nodes++;
             const float lxs[4] = {lx.x, lx.y, lx.z, lx.w}, lys[4] = {ly.x, ly.y, ly.z, ly.w}, lzs[4] = {lz.x, lz.y, lz.z, lz.w};
             const float hxs[4] = {hx.x, hx.y, hx.z, hx.w}, hys[4] = {hy.x, hy.y, hy.z, hy.w}, hzs[4] = {hz.x, hz.y, hz.z, hz.w};
@@ -325,8 +355,10 @@ struct AnyWalker4 {
         }
         if (leaf_mode) {
             const int i = ti;
-            const float4* g = ws.tris + 3 * i;
-            float4 g0 = __ldg(g), g1 = __ldg(g + 1), g2 = __ldg(g + 2);
+            const float4* g = ws.tris + kTriStride * i;
+            float4 g0, g1, g2, g3;
+            ldg_pair(g, g0, g1);
+            ldg_pair(g + 2, g2, g3);
             float t, tu, tv;
             if (Count) cnt->tris++;
             if (tri_intersect(g0, g1, g2, o, d, tmax, t, tu, tv) &&

@@ -9,12 +9,16 @@ namespace ptw {
 
 // Scene arrays on the device. Layouts (all 16-byte aligned):
 //   nodes     4 x float4 per node: (lmin, left) (lmax, lcount) (rmin, right) (rmax, rcount)
-//   tris      3 x float4 per triangle: (v0, material) (e1, flags) (e2, pad)   [BVH order]
+//   tris      kTriStride (4) x float4 per triangle: (v0, material) (e1, flags) (e2, pad) (unused)
+//             [BVH order]; 64 bytes each, so that a triangle is two aligned 256-bit loads
 //   tri_idx   int4 per triangle: (vertex 0, vertex 1, vertex 2, emissive entry or -1)
 //   normals   float4 per vertex (n, 0);  uvs float2 per vertex;  tangents float4 per vertex
 //   materials 5 x float4 per material: Photon's 80-byte Material read as five 16-byte words
 //   textures  int4 per texture: (width, height, texel offset, repeat | srgb << 1)
 //   env       float4 per texel (rgb, luminance), row_sin per row, rotation cos/sin precomputed
+// float4 records per triangle in DevScene::tris (Photon's 48-byte TriGeom padded to 64 bytes).
+constexpr int kTriStride = 4;
+
 struct DevScene {
     const float4* nodes;
     const float4* nodes4;     // the 4-wide BVH for any-hit rays (8 float4 per node), or null

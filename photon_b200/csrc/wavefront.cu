@@ -508,7 +508,7 @@ __device__ __forceinline__ uint32_t shade_key(const WfParams& P, uint32_t p, uin
     int tri = __float_as_int(P.pb.hit[i].y);
     if (tri < 0) return 0;
     const DevScene& s = scene_for(P, P.single_scene >= 0 ? 0 : int(P.pb.id[p][i].x));
-    return s.shade_keys[__float_as_int(__ldg(s.tris + 3 * tri).w)];
+    return s.shade_keys[__float_as_int(__ldg(s.tris + kTriStride * tri).w)];
 }
 
 // Persistent over the queue. Without material sorting each warp claims 32 paths in queue order. With
