@@ -258,6 +258,9 @@ typedef struct pt_tuning {
     int32_t shadow_refill;     /* the same for the shadow (any-hit) walk; <= 0 keep */
     int32_t walk_burst;        /* walk steps each lane takes between two refill checks of its warp (1 to 2^20);
                                   <= 0 keep */
+    int32_t sort_shadows;      /* 0 off (the default), 1-6: walk the shadow rays of iterations of at least
+                                  2,097,152 paths ordered by direction octant + Morton origin cell (this
+                                  many bits per axis); -1 keep */
 } pt_tuning;
 int32_t pt_set_tuning(pt_renderer* r, const pt_tuning* t);
 int32_t pt_get_tuning(const pt_renderer* r, pt_tuning* t);

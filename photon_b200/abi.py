@@ -160,7 +160,8 @@ class Tuning(C.Structure):
     _fields_ = [("path_capacity", C.c_int32), ("trace_block", C.c_int32), ("shade_block", C.c_int32),
                 ("sort_by_material", C.c_int32), ("graph_bounces", C.c_int32), ("sort_rays", C.c_int32),
                 ("packed", C.c_int32), ("tail_paths", C.c_int32), ("wide_shadows", C.c_int32),
-                ("trace_refill", C.c_int32), ("shadow_refill", C.c_int32), ("walk_burst", C.c_int32)]
+                ("trace_refill", C.c_int32), ("shadow_refill", C.c_int32), ("walk_burst", C.c_int32),
+                ("sort_shadows", C.c_int32)]
 
 
 class KernelTime(C.Structure):

@@ -113,6 +113,8 @@ void WavefrontEngine::reserve_paths(uint64_t needed) {
     pb_.sh1 = bufs_[10].ptr;
     pb_.sh2 = bufs_[11].ptr;
     keys_.allocate(want);
+    shadow_keys_.allocate(want);
+    shadow_perm_.allocate(want);
     pb_.capacity = uint32_t(want);
     if (graph_) {
         cudaGraphExecDestroy(graph_);
@@ -121,7 +123,8 @@ void WavefrontEngine::reserve_paths(uint64_t needed) {
 }
 
 size_t WavefrontEngine::device_bytes() const {
-    size_t b = ctr_.bytes();
+    size_t b = ctr_.bytes() + keys_.bytes() + hist_.bytes() + offsets_.bytes() + shadow_keys_.bytes() + shadow_hist_.bytes() +
+               shadow_offsets_.bytes() + shadow_perm_.bytes();
     for (const auto& x : bufs_) b += x.bytes();
     for (const auto& x : ids_) b += x.bytes();
     return b;
@@ -133,6 +136,13 @@ void WavefrontEngine::ensure_shape() {
         hist_.allocate(buckets);
         offsets_.allocate(buckets);
         hist_.zero(stream_);
+        PTW_CUDA(cudaStreamSynchronize(stream_));
+    }
+    if (tuning_.sort_shadows > 0 && shadow_hist_.count < (size_t(8) << (3 * tuning_.sort_shadows))) {
+        size_t buckets = size_t(8) << (3 * tuning_.sort_shadows);
+        shadow_hist_.allocate(buckets);
+        shadow_offsets_.allocate(buckets);
+        shadow_hist_.zero(stream_);
         PTW_CUDA(cudaStreamSynchronize(stream_));
     }
     if (shape_ok_) return;
@@ -161,6 +171,11 @@ WfParams WavefrontEngine::params(const DevScene* scenes, int single, const DevVi
     p.keys = keys_.ptr;
     p.hist = hist_.ptr;
     p.offsets = offsets_.ptr;
+    p.shadow_sort_bits = tuning_.sort_shadows;
+    p.shadow_keys = shadow_keys_.ptr;
+    p.shadow_hist = shadow_hist_.ptr;
+    p.shadow_offsets = shadow_offsets_.ptr;
+    p.shadow_perm = shadow_perm_.ptr;
     return p;
 }
 
@@ -210,7 +225,10 @@ void WavefrontEngine::run(const DevScene* scenes, int single_scene, const DevVie
     PTW_CUDA(cudaMemcpyAsync(ctr_.ptr, h_ctr_, sizeof(Counters), cudaMemcpyHostToDevice, stream_));
     WfParams p = params(scenes, single_scene, views, n_views, count_work || (profile_flags_ & PT_PROFILE_TRAVERSAL_COUNTS));
     // A render too small for any iteration to reach the sorting threshold launches no sort kernels.
-    if (std::min<uint64_t>(total_work, uint64_t(tuning_.path_capacity)) < kSortMinPaths) p.sort_bits = 0;
+    if (std::min<uint64_t>(total_work, uint64_t(tuning_.path_capacity)) < kSortMinPaths) {
+        p.sort_bits = 0;
+        p.shadow_sort_bits = 0;
+    }
     bool use_graph = tuning_.graph_bounces > 0;
     bool timed = (profile_flags_ & PT_PROFILE_KERNEL_TIMES) != 0;
     if (use_graph && (!graph_ || std::memcmp(&graph_params_, &p, sizeof(p)) != 0 || graph_iters_ != tuning_.graph_bounces)) capture(p);
@@ -715,6 +733,10 @@ void Renderer::set_tuning(const pt_tuning& t) {
     if (t.shadow_refill > 0) cur.shadow_refill = t.shadow_refill;
     if (t.walk_burst > (1 << 20)) throw Error{PT_ERR_INVALID, "walk_burst must be in [1, 2^20]"};
     if (t.walk_burst > 0) cur.walk_burst = t.walk_burst;
+    if (t.sort_shadows >= 0) {
+        if (t.sort_shadows > 6) throw Error{PT_ERR_INVALID, "sort_shadows must be in [0, 6]"};
+        cur.sort_shadows = t.sort_shadows;
+    }
     engine_->set_tuning(cur);
 }
 
@@ -732,6 +754,7 @@ void Renderer::get_tuning(pt_tuning* t) const {
     t->trace_refill = c.trace_refill;
     t->shadow_refill = c.shadow_refill;
     t->walk_burst = c.walk_burst;
+    t->sort_shadows = c.sort_shadows;
 }
 
 // Coordinate descent over the knobs, one at a time, each candidate timed on the same probe view set.
@@ -792,6 +815,7 @@ void Renderer::tune_on(const std::vector<pt_view>& probe, pt_tuning* chosen, dou
         try_knob([](Tuning& t, int v) { t.trace_refill = v; }, {1, 8, 16, 24, 32});
         try_knob([](Tuning& t, int v) { t.shadow_refill = v; }, {1, 8, 16, 24, 32});
         try_knob([](Tuning& t, int v) { t.walk_burst = v; }, {4, 8, 16, 32, 64});
+        try_knob([](Tuning& t, int v) { t.sort_shadows = v; }, {0, 3, 4, 5});
         engine_->set_tuning(best);
         if (tuned_rate) *tuned_rate = best_rate;
         if (chosen) get_tuning(chosen);

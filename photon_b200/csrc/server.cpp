@@ -492,7 +492,7 @@ void Server::set_tuning(const pt_tuning& t) {
     if (t.trace_refill > 0) cur.trace_refill = t.trace_refill;
     if (t.shadow_refill > 0) cur.shadow_refill = t.shadow_refill;
     if (t.walk_burst > 0) cur.walk_burst = t.walk_burst;
-    pending_tuning_ = cur;
+    pending_tuning_ = cur;  // (the shadow-queue order is not taken: the server's wavefront has no buffers for it)
     tuning_pending_ = true;
     cv_work_.notify_all();
 }

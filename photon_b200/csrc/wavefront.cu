@@ -138,6 +138,7 @@ __global__ void k_setup(const __grid_constant__ WfParams P) {
     c->tail = (tail_paths > 0 && cnt + n > 0 && cnt + n <= tail_paths && c->work_next >= c->work_total) ? 1u : 0u;
     // Sorting pays for its scan and scatter only on large iterations.
     c->sorting = (P.sort_bits > 0 && !c->tail && cnt + n >= kSortMinPaths) ? 1u : 0u;
+    c->shadow_sorting = (P.shadow_sort_bits > 0 && !c->tail && cnt + n >= kSortMinPaths) ? 1u : 0u;
     for (int k = 0; k < 6; k++) c->fetch[k] = 0;
     if (cnt + n > 0) c->iterations++;
 }
@@ -188,7 +189,7 @@ __global__ void __launch_bounds__(256) k_generate(const __grid_constant__ WfPara
 // lanes in different phases of their walks (visiting nodes, testing a leaf's triangles) proceed as
 // separate groups whose load latencies overlap, instead of meeting at a warp-wide vote every step.
 // begin(i, w, ws) initialises walker w from queue entry i (and, unless Single, sets the lane's scene
-// arrays ws); end(i, w) consumes the finished walk. Single: every ray walks `uniform`, whose array
+// arrays ws) and returns the index of the ray's record; end(record, w) consumes the finished walk. Single: every ray walks `uniform`, whose array
 // bases stay in registers for the whole loop. Count: tc.steps counts lane steps and warp_steps the
 // loop's iterations.
 template <typename W, int Overflow, bool Count, bool Single, typename Begin, typename End>
@@ -211,8 +212,7 @@ __device__ __forceinline__ void walk_queue(uint32_t n, uint32_t* claim, uint32_t
             if (!live) {
                 const uint32_t r = base + uint32_t(__popc(idle & below));
                 if (r < n) {
-                    idx = r;
-                    begin(r, w, ws);
+                    idx = begin(r, w, ws);
                     live = true;
                 }
             }
@@ -265,7 +265,11 @@ __global__ void __maxnreg__(56) k_trace(const __grid_constant__ WfParams P) {
     if (Single) {
         walk_queue<W, kStackSize - kSmemStack, Count, true>(
             n, &c->fetch[1], P.trace_refill, P.walk_burst, stack, blockDim.x, uni, tc, warp_steps,
-            [&](uint32_t i, W& w, WalkScene&) { w.init(xyz(P.pb.o[p][i]), xyz(P.pb.d[p][i]), kInf); }, end);
+            [&](uint32_t i, W& w, WalkScene&) {
+                w.init(xyz(P.pb.o[p][i]), xyz(P.pb.d[p][i]), kInf);
+                return i;
+            },
+            end);
     } else {
         walk_queue<W, kStackSize - kSmemStack, Count, false>(
             n, &c->fetch[1], P.trace_refill, P.walk_burst, stack, blockDim.x, uni, tc, warp_steps,
@@ -273,6 +277,7 @@ __global__ void __maxnreg__(56) k_trace(const __grid_constant__ WfParams P) {
                 const DevScene& s = P.scenes[P.views[P.pb.id[p][i].x].scene];
                 ws = WalkScene{s.nodes, s.tris, &s};
                 w.init(xyz(P.pb.o[p][i]), xyz(P.pb.d[p][i]), kInf);
+                return i;
             },
             end);
     }
@@ -484,6 +489,15 @@ __device__ __forceinline__ void shade_path(const WfParams& P, Counters* c, uint3
     }
     // Shadow rays: target the continuing slot, or the finished sample.
     uint32_t qs = warp_append(shadow, &c->shadow_count);
+    if (P.shadow_sort_bits > 0 && c->shadow_sorting) {
+        // Their sort key (direction octant, Morton cell of the origin) and bucket count, for the walk order.
+        const uint32_t key = shadow ? ray_key(scene_for(P, id.x), sh.o, sh.d, P.shadow_sort_bits) : 0xffffffffu;
+        const uint32_t peers = __match_any_sync(kFull, key);
+        if (shadow) {
+            P.shadow_keys[qs] = key;
+            if (int(lane_id()) == __ffs(peers) - 1) atomicAdd(&P.shadow_hist[key], uint32_t(__popc(peers)));
+        }
+    }
     if (shadow) {
         P.pb.sh0[qs] = make_float4(sh.o.x, sh.o.y, sh.o.z, sh.tmax);
         P.pb.sh1[qs] = make_float4(sh.d.x, sh.d.y, sh.d.z, __uint_as_float(cont ? slot : id.y));
@@ -653,6 +667,9 @@ __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfPar
     const uint32_t q = c->parity ^ 1u, n = c->shadow_count;
     TraversalCounters tc{0, 0, 0};
     uint32_t warp_steps = 0;
+    // Queue position -> record: the sorted order of this iteration's shadow rays, or the queue's own.
+    const bool sorted = c->shadow_sorting != 0;
+    auto record = [&](uint32_t i) { return sorted ? __ldg(P.shadow_perm + i) : i; };
     // An unoccluded shadow ray adds its contribution to its path (or to its finished sample).
     auto deliver = [&](uint32_t i) {
         const float4 cc = P.pb.sh2[i];
@@ -671,14 +688,16 @@ __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfPar
         }
     };
     auto init = [&](uint32_t i, auto& w) {
-        const float4 a = P.pb.sh0[i];
-        w.init(xyz(a), xyz(P.pb.sh1[i]), a.w);
+        const uint32_t j = record(i);
+        const float4 a = P.pb.sh0[j];
+        w.init(xyz(a), xyz(P.pb.sh1[j]), a.w);
+        return j;
     };
     if (Wide && Single && P.scenes[P.single_scene].nodes4) {
         using W4 = AnyWalker4<Count, Packed>;
         walk_queue<W4, kBvh4Stack - kSmemStack, Count, true>(
             n, &c->fetch[3], P.shadow_refill, P.walk_burst, stack, blockDim.x, single_walk_scene(P, true), tc, warp_steps,
-            [&](uint32_t i, W4& w, WalkScene&) { init(i, w); },
+            [&](uint32_t i, W4& w, WalkScene&) { return init(i, w); },
             [&](uint32_t i, const W4& w) {
                 if (!w.hit) deliver(i);
             });
@@ -689,14 +708,15 @@ __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfPar
         };
         if (Single) {
             walk_queue<W, kStackSize - kSmemStack, Count, true>(n, &c->fetch[3], P.shadow_refill, P.walk_burst, stack, blockDim.x, single_walk_scene(P, false),
-                                                                tc, warp_steps, [&](uint32_t i, W& w, WalkScene&) { init(i, w); }, end);
+                                                                tc, warp_steps, [&](uint32_t i, W& w, WalkScene&) { return init(i, w); }, end);
         } else {
             walk_queue<W, kStackSize - kSmemStack, Count, false>(
                 n, &c->fetch[3], P.shadow_refill, P.walk_burst, stack, blockDim.x, WalkScene{nullptr, nullptr, nullptr}, tc, warp_steps,
                 [&](uint32_t i, W& w, WalkScene& ws) {
-                    const DevScene& s = P.scenes[P.views[__float_as_uint(P.pb.sh2[i].w) & 0x7fffffffu].scene];
+                    const uint32_t j = init(i, w);
+                    const DevScene& s = P.scenes[P.views[__float_as_uint(P.pb.sh2[j].w) & 0x7fffffffu].scene];
                     ws = WalkScene{s.nodes, s.tris, &s};
-                    init(i, w);
+                    return j;
                 },
                 end);
         }
@@ -713,8 +733,12 @@ __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfPar
 // Exclusive scan of the bucket counts into write offsets (one block), then zero the counts. Each warp
 // takes a contiguous 32nd of the buckets and reads it 32 consecutive counts at a time (coalesced):
 // a first pass sums its part, the 32 part sums are scanned, and a second pass writes the offsets.
+// Shadow: the shadow queue's histogram (shadow_hist -> shadow_offsets), when its order is sorted.
+template <bool Shadow>
 __global__ void __launch_bounds__(1024) k_sort_scan(const __grid_constant__ WfParams P, uint32_t buckets) {
-    if (!P.ctr->sorting) return;
+    if (!(Shadow ? P.ctr->shadow_sorting : P.ctr->sorting)) return;
+    uint32_t* const hist = Shadow ? P.shadow_hist : P.hist;
+    uint32_t* const offsets = Shadow ? P.shadow_offsets : P.offsets;
     __shared__ uint32_t part[32];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t per = (buckets + 31u) / 32u;
@@ -722,7 +746,7 @@ __global__ void __launch_bounds__(1024) k_sort_scan(const __grid_constant__ WfPa
     uint32_t total = 0;
     for (uint32_t base = lo; base < hi; base += 32u) {
         const uint32_t k = base + lane;
-        uint32_t v = k < hi ? P.hist[k] : 0u;
+        uint32_t v = k < hi ? hist[k] : 0u;
         for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
         total += v;
     }
@@ -741,15 +765,15 @@ __global__ void __launch_bounds__(1024) k_sort_scan(const __grid_constant__ WfPa
     uint32_t carry = part[warp];
     for (uint32_t base = lo; base < hi; base += 32u) {
         const uint32_t k = base + lane;
-        const uint32_t v = k < hi ? P.hist[k] : 0u;
+        const uint32_t v = k < hi ? hist[k] : 0u;
         uint32_t incl = v;
         for (int off = 1; off < 32; off <<= 1) {
             const uint32_t u = __shfl_up_sync(kFull, incl, off);
             if (int(lane) >= off) incl += u;
         }
         if (k < hi) {
-            P.offsets[k] = carry + incl - v;
-            P.hist[k] = 0;
+            offsets[k] = carry + incl - v;
+            hist[k] = 0;
         }
         carry += __shfl_sync(kFull, incl, 31);
     }
@@ -779,6 +803,25 @@ __global__ void __launch_bounds__(256) k_sort_scatter(const __grid_constant__ Wf
             P.pb.lr[p][dst] = P.pb.lr[q][i];
             P.pb.id[p][dst] = P.pb.id[q][i];
         }
+    }
+}
+
+// The walk order of the shadow queue: each ray's queue position lands at its bucket's next place in
+// shadow_perm (the records themselves stay where shade wrote them).
+__global__ void __launch_bounds__(256) k_shadow_order(const __grid_constant__ WfParams P) {
+    Counters* c = P.ctr;
+    if (!c->shadow_sorting) return;
+    const uint32_t n = c->shadow_count;
+    const uint32_t warps = gridDim.x * (blockDim.x / 32u);
+    for (uint32_t i0 = (blockIdx.x * (blockDim.x / 32u) + threadIdx.x / 32u) * 32u; i0 < n; i0 += warps * 32u) {
+        const uint32_t i = i0 + lane_id();
+        const uint32_t key = i < n ? P.shadow_keys[i] : 0xffffffffu;
+        const uint32_t peers = __match_any_sync(kFull, key);
+        const int leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (i < n && int(lane_id()) == leader) base = atomicAdd(&P.shadow_offsets[key], uint32_t(__popc(peers)));
+        base = __shfl_sync(kFull, base, leader);
+        if (i < n) P.shadow_perm[base + __popc(peers & ((1u << lane_id()) - 1u))] = i;
     }
 }
 
@@ -1060,9 +1103,13 @@ cudaError_t wf_iteration(const WfParams& p, const LaunchShape& ls, cudaStream_t 
     mark(3);
     k_shade<<<ls.shade_grid, ls.shade_block, 0, stream>>>(p);
     mark(4);
+    if (p.shadow_sort_bits > 0) {
+        k_sort_scan<true><<<1, 1024, 0, stream>>>(p, 8u << (3 * p.shadow_sort_bits));
+        k_shadow_order<<<ls.gen_grid, ls.gen_block, 0, stream>>>(p);
+    }
     launch_traversal(p, ls, stream, smem, true);
     if (p.sort_bits > 0) {
-        k_sort_scan<<<1, 1024, 0, stream>>>(p, 8u << (3 * p.sort_bits));
+        k_sort_scan<false><<<1, 1024, 0, stream>>>(p, 8u << (3 * p.sort_bits));
         k_sort_scatter<<<ls.gen_grid, ls.gen_block, 0, stream>>>(p);
         k_sort_finish<<<1, 32, 0, stream>>>(p.ctr);
     }

@@ -50,6 +50,7 @@ struct Counters {
     uint32_t tail;                   // 1: this iteration finishes every queued path in k_tail
     uint32_t tail_limit;             // queued paths at or below which k_tail takes over (host-set per render)
     uint32_t sorting;                // 1: this iteration's continuing rays are sorted (sort_bits > 0, enough paths)
+    uint32_t shadow_sorting;         // 1: this iteration's shadow rays are walked in sorted order (shadow_sort_bits > 0)
     uint32_t gen_view;               // first view whose work is not all generated (views are in work order)
     uint32_t iterations;
     unsigned long long work_base, work_next, work_total;
@@ -96,6 +97,11 @@ struct WfParams {
     uint32_t* keys;            // capacity entries (sort keys of the shade output)
     uint32_t* hist;            // 8 << (3 * sort_bits) bucket counts (zero between iterations)
     uint32_t* offsets;         // bucket write positions of the scatter
+    int shadow_sort_bits;      // > 0: walk the shadow queue ordered by direction octant + Morton origin cell
+    uint32_t* shadow_keys;     // capacity entries (sort keys of the shadow queue)
+    uint32_t* shadow_hist;     // 8 << (3 * shadow_sort_bits) bucket counts (zero between iterations)
+    uint32_t* shadow_offsets;
+    uint32_t* shadow_perm;     // capacity entries: the shadow queue's order for the walk
 };
 
 // A camera passed by value to the probe kernels (pt_camera as 16 floats).
@@ -121,7 +127,9 @@ cudaError_t wf_iteration(const WfParams& p, const LaunchShape& ls, cudaStream_t 
 // coherence gains).
 constexpr uint32_t kSortMinPaths = 1u << 21;
 // Kernels wf_iteration launches for these parameters.
-inline int wf_kernels_per_iteration(const WfParams& p) { return 5 + (p.tail_paths > 0 ? 1 : 0) + (p.sort_bits > 0 ? 3 : 0); }
+inline int wf_kernels_per_iteration(const WfParams& p) {
+    return 5 + (p.tail_paths > 0 ? 1 : 0) + (p.sort_bits > 0 ? 3 : 0) + (p.shadow_sort_bits > 0 ? 2 : 0);
+}
 // Sums the samples of every pixel of a view in sample order (after a pass).
 cudaError_t wf_accumulate(const DevView* d_view, const DevView& h_view, int first_pass, int last_pass, cudaStream_t stream);
 // rgb[3 i + c] = accum[i].c * scale for n pixels (a finished image, averaged over its samples).

@@ -302,15 +302,16 @@ def test_resize_rejects_oversized_images_and_keeps_working():
 
 @pytest.mark.parametrize("bits", [3, 4, 5])
 def test_ray_sorting_is_bit_identical(bits):
-    """Ray sorting runs only on iterations of at least 2^20 paths (smaller ones do not pay for the
-    scan and scatter): a 512x288x8 frame (1.18 M paths) sorts its first bounces, and its image equals
-    the unsorted render bit for bit (sorting reorders the queue, never a path's arithmetic)."""
+    """Ray sorting (continuing rays, moved into sorted order) and the sorted walk order of the shadow
+    queue run only on iterations of at least 2^21 paths (smaller ones do not pay for the scans): a
+    640x360x16 frame (3.7 M paths in one pool) sorts its first bounces, and its image equals the render
+    with both sorts off bit for bit (sorting reorders queues, never a path's arithmetic)."""
     desc, camf, keep = scenes.scene("terrain")
-    w, h, spp = 512, 288, 8
+    w, h, spp = 640, 360, 16
     cam = camf(w / h)
     rs = _settings("terrain", w, h, seed=4)
     imgs = []
-    for t in ({}, dict(sort_rays=bits)):
+    for t in (dict(sort_rays=0, sort_shadows=0), dict(sort_rays=bits, sort_shadows=bits), dict(sort_rays=0, sort_shadows=bits)):
         r = native.Renderer()
         r.upload(desc)
         r.resize(w, h)
@@ -319,4 +320,5 @@ def test_ray_sorting_is_bit_identical(bits):
         r.render(cam, rs, spp)
         imgs.append(r.download_image())
         r.close()
-    assert np.array_equal(imgs[0].view(np.uint32), imgs[1].view(np.uint32))
+    for img in imgs[1:]:
+        assert np.array_equal(imgs[0].view(np.uint32), img.view(np.uint32))
