@@ -318,6 +318,11 @@ int32_t pt_light_picks_primary(pt_renderer* r, const pt_camera* camera, const pt
 /* BVH node visits of the primary ray through each pixel centre (heatmap_kernel,
  * gpu_renderer.cu:98-106), w * h floats. */
 int32_t pt_heatmap(pt_renderer* r, const pt_camera* camera, int32_t width, int32_t height, float* visits);
+/* Any-hit walks (traverse.h:144-147, occluded; the shadow rays' walk) of n caller rays, 8 floats each
+ * (origin, tmax, direction, unused): out4 per ray = (occluded, first triangle accepted in the walk's
+ * order or -1, node visits, triangle tests). wide = 1 walks the 4-wide BVH where the scene has one
+ * (then only `occluded` is Photon's, the counts are of the 4-wide walk). */
+int32_t pt_occlusion_probe(pt_renderer* r, const float* rays8, int32_t n, int32_t wide, int32_t* out4);
 
 /* ---- batched views (one persistent launch over many views) --------------------------------- */
 typedef struct pt_view {

@@ -52,6 +52,7 @@ def restatement():
         L.orc_trace_primary.argtypes = [P(abi.SceneDesc), P(abi.Camera), C.c_int, C.c_int, C.c_uint32, C.c_uint32, _f32p]
         L.orc_light_picks_primary.argtypes = [P(abi.SceneDesc), P(abi.Camera), P(abi.RenderSettings), C.c_uint32, _i32p]
         L.orc_heatmap.argtypes = [P(abi.SceneDesc), P(abi.Camera), C.c_int, C.c_int, _f32p]
+        L.orc_occluded.argtypes = [P(abi.SceneDesc), _f32p, C.c_int, _i32p]
         L.orc_count.argtypes = [P(abi.SceneDesc), P(abi.Camera), P(abi.RenderSettings), C.c_int, P(OrcCounters)]
         L.orc_rng_floats.argtypes = [C.c_uint64, C.c_uint64, C.c_int, _f32p]
         L.orc_hash_u32.argtypes = [C.c_uint32]
@@ -116,6 +117,7 @@ def _bind_ref(L):
     L.ref_trace_primary.argtypes = [C.c_void_p, P(abi.Camera), C.c_int, C.c_int, C.c_uint32, C.c_uint32, _f32p]
     L.ref_light_picks_primary.argtypes = [C.c_void_p, P(abi.Camera), P(abi.RenderSettings), C.c_uint32, _i32p]
     L.ref_heatmap.argtypes = [C.c_void_p, P(abi.Camera), C.c_int, C.c_int, _f32p]
+    L.ref_occluded.argtypes = [C.c_void_p, _f32p, C.c_int, _i32p]
     L.ref_alias_table.argtypes = [_f32p, C.c_int, P(abi.AliasEntry)]
     L.ref_rng_floats.argtypes = [C.c_uint64, C.c_uint64, C.c_int, _f32p]
     L.ref_offset_ray.argtypes = [C.c_int, _f32p, _f32p, _f32p]
@@ -227,6 +229,13 @@ class RefScene:
         self.lib.ref_heatmap(self.h, C.byref(cam), w, h, out)
         return out
 
+    def occluded(self, rays8):
+        """Photon's any-hit walk: (n, 4) of (occluded, accepted triangle or -1, node visits, 0)."""
+        rays8 = np.ascontiguousarray(rays8, np.float32)
+        out = np.zeros((rays8.shape[0], 4), np.int32)
+        self.lib.ref_occluded(self.h, rays8, rays8.shape[0], out)
+        return out
+
     def __del__(self):
         try:
             if self.h:
@@ -284,6 +293,15 @@ def orc_light_picks(desc, cam, rs, frame=0):
 def orc_heatmap(desc, cam, w, h):
     out = np.zeros((h, w), np.float32)
     restatement().orc_heatmap(C.byref(desc), C.byref(cam), w, h, out)
+    return out
+
+
+def orc_occluded(desc, rays8):
+    """The restatement's any-hit walk: (n, 4) of (occluded, accepted triangle or -1, node visits,
+    triangle tests)."""
+    rays8 = np.ascontiguousarray(rays8, np.float32)
+    out = np.zeros((rays8.shape[0], 4), np.int32)
+    restatement().orc_occluded(C.byref(desc), rays8, rays8.shape[0], out)
     return out
 
 

@@ -1134,6 +1134,25 @@ void orc_light_picks_primary(const pt_scene_desc* s, const pt_camera* cam, const
         }
 }
 
+void orc_occluded(const pt_scene_desc* s, const float* rays8, int n, int32_t* out4) { /* traverse.h:144-147 */
+    for (int i = 0; i < n; i++) {
+        const float* q = rays8 + 8 * (size_t)i;
+        ray_t r;
+        r.o = V3(q[0], q[1], q[2]);
+        r.tmax = q[3];
+        r.d = V3(q[4], q[5], q[6]);
+        hit_t h = {K_INF, -1, 0, 0};
+        int visits = 0;
+        trav_count c;
+        memset(&c, 0, sizeof(c));
+        int occ = traverse(s, &r, &h, 1, &visits, &c);
+        out4[4 * i] = occ;
+        out4[4 * i + 1] = occ ? h.tri : -1;
+        out4[4 * i + 2] = visits;
+        out4[4 * i + 3] = (int32_t)c.tri_tests;
+    }
+}
+
 void orc_heatmap(const pt_scene_desc* s, const pt_camera* cam, int w, int h, float* out) {
     for (int y = 0; y < h; y++)
         for (int x = 0; x < w; x++) {

@@ -47,6 +47,9 @@ void orc_light_picks_primary(const pt_scene_desc* s, const pt_camera* cam, const
 
 /* Node visits of the pixel-centre primary ray (gpu_renderer.cu:98-106). */
 void orc_heatmap(const pt_scene_desc* s, const pt_camera* cam, int w, int h, float* visits);
+/* Any-hit walks of n rays (origin, tmax, direction, unused): (occluded, first accepted triangle or -1,
+ * node visits, triangle tests) per ray. */
+void orc_occluded(const pt_scene_desc* s, const float* rays8, int n, int32_t* out4);
 
 /* Work counts of the path tracer, for the algorithmic-bytes model (rays, node visits, triangle
  * tests, alpha tests, shading events, NEE picks per group, texture taps), accumulated over every

@@ -474,6 +474,27 @@ void ref_light_picks_primary(void* h, const pt_camera* cam, const pt_render_sett
         }
 }
 
+// Photon's any-hit walk (traverse<true>, traverse.h:66-138, as occluded calls it at :144-147) of n
+// rays (origin, tmax, direction, unused): (occluded, the accepted triangle or -1, node visits, 0).
+void ref_occluded(void* h, const float* rays8, int n, int32_t* out4) {
+    RefScene& r = *static_cast<RefScene*>(h);
+    SceneView s = r.scene.view();
+    for (int i = 0; i < n; i++) {
+        const float* q = rays8 + 8 * size_t(i);
+        Ray ray;
+        ray.o = vec3(q[0], q[1], q[2]);
+        ray.tmax = q[3];
+        ray.d = vec3(q[4], q[5], q[6]);
+        Hit hit;
+        int visits = 0;
+        const bool occ = traverse<true>(s, ray, hit, &visits);
+        out4[4 * i] = occ ? 1 : 0;
+        out4[4 * i + 1] = occ ? hit.tri : -1;
+        out4[4 * i + 2] = visits;
+        out4[4 * i + 3] = 0;
+    }
+}
+
 // BVH node visits of the primary ray through each pixel centre (gpu_renderer.cu:98-106).
 void ref_heatmap(void* h, const pt_camera* cam, int w, int hgt, float* out) {
     RefScene& r = *static_cast<RefScene*>(h);

@@ -236,6 +236,11 @@ int32_t pt_get_tuning(const pt_renderer* r, pt_tuning* t) {
     return PT_OK;
 }
 
+int32_t pt_occlusion_probe(pt_renderer* r, const float* rays8, int32_t n, int32_t wide, int32_t* out4) {
+    if (!rays8 || !out4 || n < 0) return PT_ERR_INVALID;
+    PT_RENDERER_CALL(r, r->r->occlusion_probe(rays8, n, wide, out4));
+}
+
 int32_t pt_trace_primary(pt_renderer* r, const pt_camera* camera, int32_t width, int32_t height, uint32_t frame, uint32_t seed, float* hits4) {
     if (!camera || !hits4) return PT_ERR_INVALID;
     PT_RENDERER_CALL(r, r->r->trace_primary(*camera, width, height, frame, seed, hits4));

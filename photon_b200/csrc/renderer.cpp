@@ -901,6 +901,19 @@ void Renderer::heatmap(const pt_camera& cam, int w, int h, float* out) {
     PTW_CUDA(cudaStreamSynchronize(stream_));
 }
 
+void Renderer::occlusion_probe(const float* rays8, int n, int wide, int32_t* out4) {
+    if (!scene_.ready()) throw Error{PT_ERR_NO_SCENE, "probe before upload"};
+    if (n <= 0) return;
+    PTW_CUDA(cudaSetDevice(device_));
+    DeviceBuffer<float4> rays;
+    rays.upload(reinterpret_cast<const float4*>(rays8), size_t(n) * 2, stream_);
+    DeviceBuffer<int4> out;
+    out.allocate(size_t(n));
+    PTW_CUDA(wf_occlusion_probe(scene_.device_view(), rays.ptr, n, wide, out.ptr, stream_));
+    PTW_CUDA(cudaMemcpyAsync(out4, out.ptr, out.bytes(), cudaMemcpyDeviceToHost, stream_));
+    PTW_CUDA(cudaStreamSynchronize(stream_));
+}
+
 void Renderer::render_views(const pt_view* views, int n) {
     if (!scene_.ready()) throw Error{PT_ERR_NO_SCENE, "render before upload"};
     if (n < 0) throw Error{PT_ERR_INVALID, "negative view count"};

@@ -165,6 +165,7 @@ public:
     void trace_primary(const pt_camera& cam, int w, int h, uint32_t frame, uint32_t seed, float* hits4);
     void light_picks(const pt_camera& cam, const pt_render_settings& rs, uint32_t frame, int32_t* picks4);
     void heatmap(const pt_camera& cam, int w, int h, float* out);
+    void occlusion_probe(const float* rays8, int n, int wide, int32_t* out4);
 
     void set_profiling(int flags);
     void get_profile(pt_profile* out) const;

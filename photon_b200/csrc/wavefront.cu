@@ -899,6 +899,26 @@ __global__ void __launch_bounds__(128) k_heatmap(const DevScene* sp, CameraArg c
     out[size_t(y) * size_t(w) + size_t(x)] = float(tc.nodes);
 }
 
+// Any-hit walks of caller rays (occluded, traverse.h:144-147): per ray whether it is occluded, the
+// first triangle accepted (-1: none) and the node visits (BVH2 walk; the 4-wide walk's visits are of
+// its own nodes). The same walkers as the shadow kernel.
+__global__ void __launch_bounds__(128) k_occlusion_probe(const DevScene* sp, const float4* rays, int n, int wide, int4* out) {
+    extern __shared__ int smem_stack[];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const DevScene& s = *sp;
+    const float4 a = rays[2 * i], b = rays[2 * i + 1];
+    TraversalCounters tc{0, 0, 0};
+    if (wide && s.nodes4) {
+        const bool occ = occluded4<true>(s, xyz(a), xyz(b), a.w, smem_stack + threadIdx.x, blockDim.x, &tc);
+        out[i] = make_int4(occ ? 1 : 0, -1, int(tc.nodes), int(tc.tris));
+        return;
+    }
+    Hit h{kInf, -1, 0.0f, 0.0f};
+    const bool occ = traverse<true, true>(s, xyz(a), xyz(b), a.w, h, smem_stack + threadIdx.x, blockDim.x, &tc);
+    out[i] = make_int4(occ ? 1 : 0, occ ? h.tri : -1, int(tc.nodes), int(tc.tris));
+}
+
 // The light pick of the first vertex of each pixel's sample (integrator.h:199-209).
 __global__ void __launch_bounds__(128) k_light_picks(const DevScene* sp, const DevView* vp, int4* out) {
     extern __shared__ int smem_stack[];
@@ -1158,6 +1178,13 @@ cudaError_t wf_light_picks(const DevScene* scene, const DevView* view, int4* out
     dim3 grid((w + 15) / 16, (h + 7) / 8);
     size_t smem = size_t(kSmemStack) * 128 * sizeof(int);
     k_light_picks<<<grid, 128, smem, stream>>>(scene, view, out);
+    return cudaGetLastError();
+}
+
+cudaError_t wf_occlusion_probe(const DevScene* scene, const float4* rays, int n, int wide, int4* out, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    const size_t smem = size_t(kSmemStack) * 128 * sizeof(int);
+    k_occlusion_probe<<<(n + 127) / 128, 128, smem, stream>>>(scene, rays, n, wide, out);
     return cudaGetLastError();
 }
 

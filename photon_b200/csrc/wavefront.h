@@ -141,6 +141,9 @@ cudaError_t wf_trace_primary(const DevScene* scene, const float* cam16, int w, i
                              float4* out, cudaStream_t stream);
 cudaError_t wf_light_picks(const DevScene* scene, const DevView* view, int4* out, int w, int h, cudaStream_t stream);
 cudaError_t wf_heatmap(const DevScene* scene, const float* cam16, int w, int h, float* out, cudaStream_t stream);
+// Any-hit walks of n rays (2 float4 each: origin + tmax, direction + unused): out[i] = (occluded,
+// first accepted triangle or -1, node visits, triangle tests).
+cudaError_t wf_occlusion_probe(const DevScene* scene, const float4* rays, int n, int wide, int4* out, cudaStream_t stream);
 
 struct DisplayParams {
     int w, h, mode;

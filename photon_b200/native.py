@@ -71,6 +71,7 @@ def _load():
         "pt_trace_primary": ([C.c_void_p, P(abi.Camera), C.c_int32, C.c_int32, C.c_uint32, C.c_uint32, _f32p], C.c_int32),
         "pt_light_picks_primary": ([C.c_void_p, P(abi.Camera), P(abi.RenderSettings), C.c_uint32, _i32p], C.c_int32),
         "pt_heatmap": ([C.c_void_p, P(abi.Camera), C.c_int32, C.c_int32, _f32p], C.c_int32),
+        "pt_occlusion_probe": ([C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p], C.c_int32),
         "pt_render_views": ([C.c_void_p, P(abi.View), C.c_int32], C.c_int32),
         "pt_download_view": ([C.c_void_p, C.c_int32, _f32p, C.c_size_t], C.c_int32),
         "pt_svgf_create": ([C.c_int32, C.c_int32, C.c_int32, P(C.c_void_p)], C.c_int32),
@@ -292,6 +293,14 @@ class Renderer:
     def heatmap(self, cam, w, h):
         out = np.zeros((h, w), np.float32)
         _check(lib.pt_heatmap(self.h, C.byref(cam), w, h, out), self._err)
+        return out
+
+    def occlusion_probe(self, rays8, wide=False):
+        """Any-hit walks of (n, 8) float32 rays (origin, tmax, direction, unused): (n, 4) int32 of
+        (occluded, first accepted triangle or -1, node visits, triangle tests)."""
+        rays8 = np.ascontiguousarray(rays8, np.float32)
+        out = np.zeros((rays8.shape[0], 4), np.int32)
+        _check(lib.pt_occlusion_probe(self.h, rays8.ctypes.data, rays8.shape[0], 1 if wide else 0, out.ctypes.data), self._err)
         return out
 
     def render_views(self, views):

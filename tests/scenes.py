@@ -20,3 +20,19 @@ def scene(name):
     if name in ("cornell", "materials", "glass", "furnace"):
         return photon_builtin(name)
     return generated(name)
+
+
+def random_rays(desc, n, seed=0):
+    """(n, 8) float32 rays for any-hit walks: origins uniform in the scene box, directions uniform on
+    the sphere, tmax infinite for half of them and uniform in (0, the box's diagonal) for the rest."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    lo = np.array([desc.bounds_min.x, desc.bounds_min.y, desc.bounds_min.z], np.float64)
+    hi = np.array([desc.bounds_max.x, desc.bounds_max.y, desc.bounds_max.z], np.float64)
+    o = lo + (hi - lo) * rng.random((n, 3))
+    d = rng.standard_normal((n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    tmax = np.where(rng.random(n) < 0.5, np.inf, rng.random(n) * np.linalg.norm(hi - lo))
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3], rays[:, 3], rays[:, 4:7] = o, tmax, d
+    return rays

@@ -272,3 +272,23 @@ def test_reference_build_holds_the_same_scene_generator(kind, tris):
         v0, v1 = getattr(c0, f), getattr(c1, f)
         assert max(abs(v0.x - v1.x), abs(v0.y - v1.y), abs(v0.z - v1.z)) < 1e-6, f
     assert abs(c0.tan_half_fov - c1.tan_half_fov) < 1e-6 and c0.aspect == c1.aspect
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["materials", "terrain"])
+def test_restatement_any_hit_walk_equals_photons(name):
+    """The any-hit walk (Photon's occluded, traverse.h:144-147): on random rays, the restatement's
+    answer, the triangle it accepts first and its node visits equal Photon's traverse<true>, including
+    rays through the terrain's alpha-masked (25%) materials."""
+    import scenes
+    if name == "terrain":
+        g = native.terrain_scene()
+        b = g.build()
+        ref = O.RefScene.from_desc(b.desc)
+    else:
+        ref = O.RefScene.builtin(name)
+    rays = scenes.random_rays(ref.desc, 20000, seed=3)
+    theirs = ref.occluded(rays)
+    ours = O.orc_occluded(ref.desc, rays)
+    assert np.array_equal(ours[:, :3], theirs[:, :3])
+    assert 0.2 < ours[:, 0].mean() < 0.95
