@@ -62,3 +62,35 @@ def test_null_arguments_are_rejected():
     assert native.lib.pt_resize(None, 1, 1) == abi.PT_ERR_INVALID
     assert native.lib.pt_server_submit(None, None, None) == abi.PT_ERR_INVALID
     native.lib.pt_destroy(None)
+
+
+def test_ctypes_mirrors_match_the_header(tmp_path):
+    """Every ctypes structure of photon_b200.abi has the size and field offsets that a C compiler gives
+    the header's struct of the same name (compiled here with gcc)."""
+    import shutil
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        import pytest
+        pytest.skip("no C compiler")
+    mirrors = {
+        "pt_tuning": abi.Tuning, "pt_profile": abi.Profile, "pt_kernel_time": abi.KernelTime, "pt_server_config": abi.ServerConfig,
+        "pt_request": abi.Request, "pt_request_stats": abi.RequestStats, "pt_server_stats": abi.ServerStats, "pt_view": abi.View,
+        "pt_stats": abi.Stats, "pt_scene_desc": abi.SceneDesc, "pt_raw_scene": abi.RawScene, "pt_texture_desc": abi.TextureDesc,
+        "pt_bvh_build_options": abi.BvhBuildOptions, "pt_light_update": abi.LightUpdate,
+    }
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "photon_wavefront.h"', "int main(void) {"]
+    for cname, ct in mirrors.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in ct._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c99", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, ct in mirrors.items():
+        assert got[(cname, "size")] == C.sizeof(ct), cname
+        for fname, _ in ct._fields_:
+            assert got[(cname, fname)] == getattr(ct, fname).offset, (cname, fname)
