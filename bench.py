@@ -329,8 +329,8 @@ def systems_sections(r, g, desc, rank):
                                  "scenes of 36 / 262,144 / 1,048,576 / 4,194,304 triangles, 150 GB budget",
                      "served": served, "plain": plain, "budget_bytes": budget,
                      "served_over_plain": served["msamples_per_s"] / plain["msamples_per_s"]}
-    # Eight real-time SVGF sessions served by the same server alongside the same stream (sessions as
-    # a request class sharing the path pool), and the same sessions on renderers of their own.
+    # Eight real-time SVGF sessions served by the same server alongside the same stream (the server's
+    # session lane), and the same sessions on renderers of their own.
     server = native.Server(budget_bytes=budget)
     sids = [server.add_scene(d) for d in descs]
     serving.run_served(server, warm)

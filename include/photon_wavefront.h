@@ -488,13 +488,15 @@ int32_t pt_server_get_stats(pt_server* s, pt_server_stats* out);
  * 379-401, as a request class of the server). A session holds a G-buffer and a denoiser history on
  * the server's device (counted against its budget). Each frame is one path per pixel of `camera`
  * (sample index = the session's frame number, seed and path options from `settings`), whose first
- * vertex writes the G-buffer and the denoiser's records (reprojection into `previous`), rendered in
- * the shared path pool with every other request in flight, then denoised by SVGF (temporal, variance,
- * `atrous_iterations` a-trous passes) with the session's history. The result is the denoised image:
- * pt_server_poll / wait / fetch take the returned request id as for any request; it equals the image
- * of the same frame sequence through pt_render_denoised. A session's frames are rendered one at a
- * time in submission order (a frame waits for its predecessor's denoise); they are not held back by
- * max_active. Closing a session cancels its frames still waiting; one on the device finishes first. */
+ * vertex writes the G-buffer and the denoiser's records (reprojection into `previous`), then denoised
+ * by SVGF (temporal, variance, `atrous_iterations` a-trous passes) with the session's history. Frames
+ * go through a lane of their own: the waiting frames of all sessions are rendered together by a second
+ * wavefront on a stream of the device's highest priority, beside the request stream, so a frame does
+ * not wait for the requests' bounce iterations. The result is the denoised image: pt_server_poll /
+ * wait / fetch take the returned request id as for any request; it equals the image of the same frame
+ * sequence through pt_render_denoised. A session's frames are rendered one at a time in submission
+ * order (a frame waits for its predecessor's denoise). Closing a session cancels its frames still
+ * waiting; one on the device finishes first. */
 int32_t pt_server_open_session(pt_server* s, int32_t scene_id, int32_t width, int32_t height, const pt_svgf_settings* svgf,
                                int32_t* session_id);
 int32_t pt_server_submit_frame(pt_server* s, int32_t session_id, const pt_camera* camera, const pt_camera* previous,

@@ -122,6 +122,17 @@ void WavefrontEngine::reserve_paths(uint64_t needed) {
     }
 }
 
+void WavefrontEngine::release_paths() {
+    if (graph_) {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+    for (auto& b : bufs_) b.release();
+    for (auto& b : ids_) b.release();
+    for (DeviceBuffer<uint32_t>* b : {&keys_, &hist_, &offsets_, &shadow_keys_, &shadow_hist_, &shadow_offsets_, &shadow_perm_}) b->release();
+    pb_ = PathBuffers{};
+}
+
 size_t WavefrontEngine::device_bytes() const {
     size_t b = ctr_.bytes() + keys_.bytes() + hist_.bytes() + offsets_.bytes() + shadow_keys_.bytes() + shadow_hist_.bytes() +
                shadow_offsets_.bytes() + shadow_perm_.bytes();

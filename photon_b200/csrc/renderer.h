@@ -57,6 +57,8 @@ public:
 
     // Makes sure the pool holds at least min(capacity, needed) paths.
     void reserve_paths(uint64_t needed);
+    // Frees the path pool and the sort buffers (the next run allocates them again).
+    void release_paths();
 
     // Renders one pass: every work item of `views` (device table of n views, work ranges
     // contiguous from 0) until all paths finished. scenes: device table; single_scene >= 0 when

@@ -81,6 +81,16 @@ Server::Server(const pt_server_config& cfg) : cfg_(cfg), device_(cfg.device) {
         }
     }
     PTW_CUDA(cudaStreamCreateWithFlags(&fin_stream_, cudaStreamNonBlocking));
+    {
+        int least = 0, greatest = 0;
+        PTW_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        PTW_CUDA(cudaStreamCreateWithPriority(&session_stream_, cudaStreamNonBlocking, greatest));
+        session_engine_ = std::make_unique<WavefrontEngine>(device_, session_stream_);
+        Tuning st;
+        st.path_capacity = 1 << 23;  // grown on the first frames to what they need, up to this
+        session_engine_->set_tuning(st);
+        lane_idle_bytes_ = session_engine_->device_bytes();
+    }
     for (Batch& b : batch_) {
         PTW_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&b.ctr), sizeof(Counters), cudaHostAllocDefault));
         PTW_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&b.work_total), sizeof(unsigned long long), cudaHostAllocDefault));
@@ -92,6 +102,7 @@ Server::Server(const pt_server_config& cfg) : cfg_(cfg), device_(cfg.device) {
     st_.budget_bytes = cfg.budget_bytes;
     if (cfg_.budget_bytes && pool_bytes_ > cfg_.budget_bytes) throw Error{PT_ERR_BUDGET, "the path pool alone exceeds the budget"};
     thread_ = std::thread([this] { loop(); });
+    session_thread_ = std::thread([this] { session_loop(); });
 }
 
 Server::~Server() {
@@ -100,8 +111,11 @@ Server::~Server() {
         stop_ = true;
     }
     cv_work_.notify_all();
+    cv_frames_.notify_all();
     if (thread_.joinable()) thread_.join();
+    if (session_thread_.joinable()) session_thread_.join();
     cudaSetDevice(device_);
+    cudaStreamSynchronize(session_stream_);
     cudaStreamSynchronize(stream_);
     cudaStreamSynchronize(fin_stream_);
     for (auto& kv : requests_) release_buffers(*kv.second, stream_);
@@ -119,10 +133,12 @@ Server::~Server() {
     }
     requests_.clear();
     sessions_.clear();
+    session_engine_.reset();
     engine_.reset();
     scenes_.clear();
     if (mem_pool_) cudaMemPoolDestroy(mem_pool_);
     cudaStreamDestroy(fin_stream_);
+    cudaStreamDestroy(session_stream_);
     cudaStreamDestroy(stream_);
 }
 
@@ -352,11 +368,12 @@ int32_t Server::open_session(int32_t scene_id, int w, int h, const pt_svgf_setti
     PTW_CUDA(cudaSetDevice(device_));
     for (DeviceBuffer<float4>* b : {&s->albedo, &s->normal_depth, &s->emission, &s->color, &s->edge, &s->motion, &s->denoised}) {
         b->allocate(npix);
-        PTW_CUDA(cudaMemsetAsync(b->ptr, 0, npix * sizeof(float4), fin_stream_));
+        PTW_CUDA(cudaMemsetAsync(b->ptr, 0, npix * sizeof(float4), session_stream_));
     }
-    s->svgf = std::make_unique<SvgfDenoiser>(device_, fin_stream_);
+    s->svgf = std::make_unique<SvgfDenoiser>(device_, session_stream_);
     s->svgf->resize(w, h);
     s->bytes = 7 * npix * sizeof(float4) + s->svgf->device_bytes();
+    // (The session lane's path pool, grown with the first frames, counts in the server's pool bytes.)
     std::lock_guard<std::mutex> g(mu_);
     if (cfg_.budget_bytes && bytes_in_use_ + s->bytes + pool_bytes_ + scene_bytes_ > cfg_.budget_bytes)
         throw Error{PT_ERR_BUDGET, "session: does not fit the device-memory budget"};
@@ -381,7 +398,7 @@ void Server::session_frame_ended(Request& r) {
     r.ses = nullptr;
     s->busy = false;
     free_session_if_closed(*s);
-    cv_work_.notify_all();  // its next frame may be admitted
+    cv_frames_.notify_all();  // its next frame may go
 }
 
 void Server::close_session(int32_t session) {
@@ -390,8 +407,8 @@ void Server::close_session(int32_t session) {
     if (it == sessions_.end() || it->second->closed) throw Error{PT_ERR_NOT_FOUND, "unknown session"};
     Session& s = *it->second;
     s.closed = true;
-    // Frames still waiting for admission end cancelled; a frame on the device finishes first.
-    for (auto q = queue_.begin(); q != queue_.end();) {
+    // Frames still waiting end cancelled; a frame on the device finishes first.
+    for (auto q = frame_queue_.begin(); q != frame_queue_.end();) {
         Request& r = *requests_[*q];
         if (r.session != session) {
             ++q;
@@ -400,7 +417,7 @@ void Server::close_session(int32_t session) {
         r.state = PT_REQ_CANCELLED;
         r.done_s = now();
         st_.cancelled++;
-        q = queue_.erase(q);
+        q = frame_queue_.erase(q);
     }
     cv_done_.notify_all();
     free_session_if_closed(s);
@@ -434,10 +451,151 @@ uint64_t Server::submit_frame(int32_t session, const pt_camera& cam, const pt_ca
     }
     const uint64_t id = q->id;
     requests_[id] = std::move(q);
-    queue_.push_back(id);
+    frame_queue_.push_back(id);
     st_.submitted++;
-    cv_work_.notify_all();
+    cv_frames_.notify_all();
     return id;
+}
+
+// The session lane's thread: takes the oldest waiting frame of every session (a session's next frame
+// waits for this one: its denoiser history), renders them together as one batched wavefront pass on
+// the session stream (their paths share that lane's pool; the tail kernel finishes the last ones),
+// then per frame sums its sample, denoises it with its session's history and resolves the image into
+// a device result buffer.
+void Server::session_loop() {
+    cudaSetDevice(device_);
+    std::unique_lock<std::mutex> lk(mu_);
+    while (!stop_) {
+        std::vector<Request*> frames;
+        size_t need = 0;
+        for (uint64_t id : frame_queue_) {
+            Request& r = *requests_[id];
+            bool taken = false;
+            for (const Request* f : frames) taken = taken || f->session == r.session;
+            auto it = sessions_.find(r.session);
+            if (taken || it == sessions_.end()) continue;
+            if (cfg_.budget_bytes && bytes_in_use_ + need + r.bytes + pool_bytes_ + scene_bytes_ > cfg_.budget_bytes) break;
+            r.ses = it->second.get();
+            frames.push_back(&r);
+            need += r.bytes;
+        }
+        if (frames.empty()) {
+            if (sessions_.empty() && lane_bytes_ > 0) {
+                // No session left: give the lane's path pool back (the next session's frames grow it again).
+                session_engine_->release_paths();
+                pool_bytes_ -= lane_bytes_;
+                lane_bytes_ = 0;
+            }
+            cv_frames_.wait_for(lk, std::chrono::milliseconds(20));
+            continue;
+        }
+        for (Request* r : frames) {
+            frame_queue_.erase(std::find(frame_queue_.begin(), frame_queue_.end(), r->id));
+            r->state = PT_REQ_RUNNING;
+            r->admit_s = now();
+            r->ses->busy = true;
+        }
+        bytes_in_use_ += need;
+        std::vector<DevScene> table;
+        for (const auto& s : scenes_) table.push_back(s->view());
+        lk.unlock();
+
+        std::string failure;
+        try {
+            std::vector<DevView> views(frames.size());
+            uint64_t work = 0;
+            int single = frames.front()->req.scene_id;
+            for (size_t k = 0; k < frames.size(); k++) {
+                Request& r = *frames[k];
+                Session& ses = *r.ses;
+                const size_t npix = size_t(r.req.width) * size_t(r.req.height);
+                if (r.req.scene_id != single) single = -1;
+                PTW_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r.sample_out), npix * sizeof(float4), mem_pool_, session_stream_));
+                PTW_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r.accum), npix * sizeof(float4), mem_pool_, session_stream_));
+                PTW_CUDA(cudaMemsetAsync(r.accum, 0, npix * sizeof(float4), session_stream_));
+                // pt_render_denoised's frame: one path per pixel whose first vertex writes the G-buffer
+                // and the denoiser's records; the sample index is the frame number.
+                DevView& v = views[k];
+                std::memset(&v, 0, sizeof(v));
+                std::memcpy(v.cam, &r.req.camera, sizeof(v.cam));
+                v.width = r.req.width;
+                v.height = r.req.height;
+                v.spp = 1;
+                v.scene = r.req.scene_id;
+                v.seed = r.req.seed;
+                v.frame0 = r.frame;
+                v.max_depth = r.req.path.max_depth;
+                v.rr_depth = r.req.path.rr_depth;
+                v.nee = r.req.path.nee;
+                v.clamp = r.req.path.clamp;
+                v.sample_out = r.sample_out;
+                v.accum = r.accum;
+                v.gbuffer = 1;
+                v.realtime = 1;
+                v.g_albedo = ses.albedo.ptr;
+                v.g_normal_depth = ses.normal_depth.ptr;
+                v.g_emission = ses.emission.ptr;
+                v.g_color = ses.color.ptr;
+                v.g_edge = ses.edge.ptr;
+                v.g_motion = ses.motion.ptr;
+                static_assert(sizeof(v.prev_cam) == sizeof(pt_camera), "camera layout");
+                std::memcpy(v.prev_cam, &r.prev, sizeof(v.prev_cam));
+                v.has_prev = 1;
+                v.work_begin = work;
+                v.work_count = npix;
+                work += npix;
+            }
+            if (session_scenes_.count < table.size()) session_scenes_.allocate(std::max<size_t>(table.size(), 16));
+            if (session_views_.count < views.size()) session_views_.allocate(std::max<size_t>(views.size(), 16));
+            PTW_CUDA(cudaMemcpyAsync(session_scenes_.ptr, table.data(), table.size() * sizeof(DevScene), cudaMemcpyHostToDevice,
+                                     session_stream_));
+            PTW_CUDA(cudaMemcpyAsync(session_views_.ptr, views.data(), views.size() * sizeof(DevView), cudaMemcpyHostToDevice,
+                                     session_stream_));
+            session_engine_->run(session_scenes_.ptr, single, session_views_.ptr, int(views.size()), work);
+            for (size_t k = 0; k < frames.size(); k++) {
+                Request& r = *frames[k];
+                Session& ses = *r.ses;
+                const uint32_t npix = uint32_t(r.req.width) * uint32_t(r.req.height);
+                PTW_CUDA(wf_accumulate(session_views_.ptr + k, views[k], 1, 1, session_stream_));  // writes the colour
+                ses.svgf->run_frame(reinterpret_cast<const float*>(ses.color.ptr), reinterpret_cast<const float*>(ses.albedo.ptr),
+                                    reinterpret_cast<const float*>(ses.emission.ptr), reinterpret_cast<const float*>(ses.edge.ptr),
+                                    reinterpret_cast<const float*>(ses.motion.ptr), ses.sv, reinterpret_cast<float*>(ses.denoised.ptr));
+                r.result_bytes = size_t(npix) * 3 * sizeof(float);
+                PTW_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r.result), r.result_bytes, mem_pool_, session_stream_));
+                PTW_CUDA(wf_resolve(ses.denoised.ptr, npix, 1.0f, false, r.result, session_stream_));
+                release_buffers(r, session_stream_);
+            }
+            PTW_CUDA(cudaStreamSynchronize(session_stream_));
+        } catch (const Error& e) {
+            failure = e.message;
+            cudaStreamSynchronize(session_stream_);
+            cudaGetLastError();
+        }
+
+        lk.lock();
+        size_t lane = session_engine_->device_bytes() - lane_idle_bytes_;
+        pool_bytes_ = pool_bytes_ - lane_bytes_ + lane;
+        lane_bytes_ = lane;
+        for (Request* r : frames) {
+            bytes_in_use_ -= r->bytes;
+            r->done_s = now();
+            if (!failure.empty() || r->cancel) {
+                release_buffers(*r, session_stream_);
+                if (r->result) cudaFreeAsync(r->result, session_stream_);
+                r->result = nullptr;
+                r->state = failure.empty() ? PT_REQ_CANCELLED : PT_REQ_FAILED;
+                r->error = failure;
+                if (failure.empty()) st_.cancelled++;
+            } else {
+                r->state = PT_REQ_DONE;
+                bytes_in_use_ += r->result_bytes;  // its result, until fetched
+                st_.completed++;
+                st_.samples_done += r->work;
+            }
+            session_frame_ended(*r);
+        }
+        cv_done_.notify_all();
+    }
 }
 
 void Server::cancel(uint64_t id) {
@@ -447,6 +605,7 @@ void Server::cancel(uint64_t id) {
     Request& r = *it->second;
     if (r.state == PT_REQ_QUEUED) {
         queue_.erase(std::remove(queue_.begin(), queue_.end(), id), queue_.end());
+        frame_queue_.erase(std::remove(frame_queue_.begin(), frame_queue_.end(), id), frame_queue_.end());
         r.state = PT_REQ_CANCELLED;
         r.done_s = now();
         st_.cancelled++;
@@ -520,22 +679,10 @@ void Server::release_buffers(Request& r, cudaStream_t s) {
 
 // Called with the lock held: allocates the request's buffers and its finished-path counter. Its work
 // is handed to the wavefront later, chunk by chunk (append_chunks).
-Server::Admit Server::try_admit(Request& r) {
-    Session* ses = nullptr;
-    if (r.session >= 0) {
-        // Session frames run one at a time per session, and are not held back by the limit on
-        // requests at once (they are small, and latency is their point).
-        auto it = sessions_.find(r.session);
-        if (it == sessions_.end()) return kSkipped;  // (closing a session cancels its queued frames)
-        ses = it->second.get();
-        if (ses->busy) return kSkipped;
-    } else {
-        const int max_active = cfg_.max_active > 0 ? cfg_.max_active : (cfg_.max_active == 0 ? kDefaultMaxActive : 0);
-        int requests = 0;
-        for (uint64_t id : active_) requests += requests_[id]->session < 0 ? 1 : 0;
-        if (max_active > 0 && requests >= max_active) return kBlocked;
-    }
-    if (cfg_.budget_bytes && bytes_in_use_ + r.bytes + pool_bytes_ + scene_bytes_ > cfg_.budget_bytes) return kBlocked;
+bool Server::try_admit(Request& r) {
+    const int max_active = cfg_.max_active > 0 ? cfg_.max_active : (cfg_.max_active == 0 ? kDefaultMaxActive : 0);
+    if (max_active > 0 && int(active_.size()) >= max_active) return false;
+    if (cfg_.budget_bytes && bytes_in_use_ + r.bytes + pool_bytes_ + scene_bytes_ > cfg_.budget_bytes) return false;
     size_t npix = size_t(r.req.width) * size_t(r.req.height);
     try {
         if (inject_failures_ > 0) {
@@ -553,7 +700,7 @@ Server::Admit Server::try_admit(Request& r) {
         r.error = e.message;
         r.done_s = now();
         cv_done_.notify_all();
-        return kAdmitted;  // consumed (failed), not retried
+        return true;  // consumed (failed), not retried
     }
     // Grow the finished-path counters by doubling.
     if (size_t(done_slots_) + 1 > d_done_.count) {
@@ -587,30 +734,12 @@ Server::Admit Server::try_admit(Request& r) {
     v.clamp = r.req.path.clamp;
     v.sample_out = r.sample_out;
     v.accum = r.accum;
-    if (ses) {
-        // The frame's first vertex writes the session's G-buffer and the denoiser's records, as
-        // pt_render_denoised's frame does; its sample index is the frame number.
-        v.frame0 = r.frame;
-        v.gbuffer = 1;
-        v.realtime = 1;
-        v.g_albedo = ses->albedo.ptr;
-        v.g_normal_depth = ses->normal_depth.ptr;
-        v.g_emission = ses->emission.ptr;
-        v.g_color = ses->color.ptr;
-        v.g_edge = ses->edge.ptr;
-        v.g_motion = ses->motion.ptr;
-        static_assert(sizeof(v.prev_cam) == sizeof(pt_camera), "camera layout");
-        std::memcpy(v.prev_cam, &r.prev, sizeof(v.prev_cam));
-        v.has_prev = 1;
-        ses->busy = true;
-        r.ses = ses;
-    }
     v.done_counter = d_done_.ptr + r.done_slot;
     bytes_in_use_ += r.bytes;
     r.state = PT_REQ_RUNNING;
     r.admit_s = now();
     active_.push_back(r.id);
-    return kAdmitted;
+    return true;
 }
 
 // Called with the lock held: hands chunks of the running requests' work to the wavefront, shortest
@@ -655,25 +784,11 @@ void Server::loop() {
         std::vector<Request*> done;      // requests whose image has landed in host memory this turn
         try {
             // Admission in arrival order while the budget allows, then chunks of work.
-            // Admission in arrival order: a request that does not fit holds back the requests behind
-            // it, but not session frames (which wait only for their own session's previous frame).
-            bool held = false;
-            for (auto q = queue_.begin(); q != queue_.end();) {
-                Request& r = *requests_[*q];
-                if (held && r.session < 0) {
-                    ++q;
-                    continue;
-                }
-                const Admit a = try_admit(r);
-                if (a == kAdmitted) {
-                    q = queue_.erase(q);
-                    continue;
-                }
-                if (a == kBlocked) {
-                    if (r.session >= 0) break;  // the budget: nothing behind it fits either
-                    held = true;
-                }
-                ++q;
+            // Admission in arrival order while the budget and the limit on requests at once allow.
+            while (!queue_.empty()) {
+                Request& r = *requests_[queue_.front()];
+                if (!try_admit(r)) break;
+                queue_.pop_front();
             }
             append_chunks();
             if (scenes_dirty_) upload_scene_table();
@@ -805,18 +920,7 @@ void Server::loop() {
                     r->result_bytes = size_t(npix) * (3 * sizeof(float) + (r->req.display ? sizeof(uint32_t) : 0));
                     PTW_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r->result), r->result_bytes, mem_pool_, fin_stream_));
                     float* rgb = r->result;
-                    if (r->ses) {
-                        // A session frame: the accumulate step above wrote its colour; denoise it with
-                        // the session's history (on this stream, in the session's frame order) and
-                        // hand out the denoised image.
-                        Session& ses = *r->ses;
-                        ses.svgf->run_frame(reinterpret_cast<const float*>(ses.color.ptr), reinterpret_cast<const float*>(ses.albedo.ptr),
-                                            reinterpret_cast<const float*>(ses.emission.ptr), reinterpret_cast<const float*>(ses.edge.ptr),
-                                            reinterpret_cast<const float*>(ses.motion.ptr), ses.sv, reinterpret_cast<float*>(ses.denoised.ptr));
-                        PTW_CUDA(wf_resolve(ses.denoised.ptr, npix, 1.0f, false, rgb, fin_stream_));
-                    } else {
-                        PTW_CUDA(wf_resolve(r->accum, npix, 1.0f / float(r->req.spp), true, rgb, fin_stream_));
-                    }
+                    PTW_CUDA(wf_resolve(r->accum, npix, 1.0f / float(r->req.spp), true, rgb, fin_stream_));
                     if (r->req.display) {
                         // The colour view of pt_display on the summed samples, after the float image.
                         DisplayParams dp{};
@@ -873,7 +977,6 @@ void Server::loop() {
                 r->done_s = now();
                 bytes_in_use_ -= r->bytes;
                 st_.cancelled++;
-                session_frame_ended(*r);
             }
             for (Request* r : done) {
                 r->state = PT_REQ_DONE;
@@ -882,7 +985,6 @@ void Server::loop() {
                 bytes_in_use_ += r->result_bytes;  // its result, until fetched
                 st_.completed++;
                 st_.samples_done += r->work;
-                session_frame_ended(*r);
             }
             if (!done.empty() || !cancelled.empty()) cv_done_.notify_all();
             release_batch_refs(released);
@@ -910,7 +1012,6 @@ void Server::loop() {
                 bytes_in_use_ += r->result_bytes;
                 st_.completed++;
                 st_.samples_done += r->work;
-                session_frame_ended(*r);
             }
             for (Finishing& f : finishing_) {
                 cudaEventDestroy(f.ev);
@@ -921,7 +1022,6 @@ void Server::loop() {
                 bytes_in_use_ -= f.r->bytes;
                 if (f.r->result) cudaFreeAsync(f.r->result, fin_stream_);
                 f.r->result = nullptr;
-                session_frame_ended(*f.r);
             }
             finishing_.clear();
             // A device failure fails every running request; the server keeps its handle valid.
@@ -931,7 +1031,6 @@ void Server::loop() {
                     release_buffers(r, stream_);
                     continue;
                 }
-                session_frame_ended(r);
                 r.state = PT_REQ_FAILED;
                 r.error = e.message;
                 r.done_s = now();

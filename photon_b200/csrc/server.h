@@ -51,7 +51,7 @@ private:
     struct Session {
         int id = 0, scene = 0, w = 0, h = 0;
         pt_svgf_settings sv{};
-        std::unique_ptr<SvgfDenoiser> svgf;  // on the finishing stream
+        std::unique_ptr<SvgfDenoiser> svgf;  // on the session stream
         DeviceBuffer<float4> albedo, normal_depth, emission, color, edge, motion, denoised;
         uint32_t frames = 0;  // frames submitted: the next frame's sample index
         bool busy = false;    // a frame is admitted and not finished
@@ -93,10 +93,10 @@ private:
     };
 
     void loop();
+    void session_loop();
     double now() const;
     size_t request_bytes(const pt_request& r) const;
-    enum Admit { kAdmitted, kBlocked, kSkipped };
-    Admit try_admit(Request& r);
+    bool try_admit(Request& r);
     void session_frame_ended(Request& r);  // with the lock held: the session may take its next frame
     void free_session_if_closed(Session& s);
     void append_chunks();
@@ -123,6 +123,16 @@ private:
     std::map<uint64_t, std::unique_ptr<Request>> requests_;
     std::map<int32_t, std::unique_ptr<Session>> sessions_;
     int32_t next_session_ = 1;
+    // The session lane: session frames are rendered by a wavefront of their own on a stream of the
+    // device's highest priority, driven by their own thread, so that a frame does not wait for the
+    // request stream's bounce iterations (which hold the whole path pool at saturation).
+    std::deque<uint64_t> frame_queue_;
+    std::condition_variable cv_frames_;
+    std::thread session_thread_;
+    cudaStream_t session_stream_ = nullptr;
+    std::unique_ptr<WavefrontEngine> session_engine_;
+    DeviceBuffer<DevScene> session_scenes_;
+    DeviceBuffer<DevView> session_views_;
     std::deque<uint64_t> queue_;
     std::vector<uint64_t> active_;
     uint64_t next_id_ = 1;
@@ -166,7 +176,9 @@ private:
     size_t views_uploaded_ = 0;
     uint64_t work_total_ = 0;
     size_t bytes_in_use_ = 0;
-    size_t pool_bytes_ = 0;
+    size_t pool_bytes_ = 0;         // the request pool and, while sessions run, the session lane's (lane_bytes_)
+    size_t lane_bytes_ = 0;         // the session lane's path pool and sort buffers
+    size_t lane_idle_bytes_ = 0;    // the lane engine's own buffers (its counters), not counted
     bool engine_started_ = false;
     int inject_failures_ = 0;
     bool tuning_pending_ = false;  // under mu_: pending_tuning_ waits for the loop

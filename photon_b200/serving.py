@@ -52,7 +52,7 @@ def run_served(server, stream, timeout_s=600.0):
 
 def run_sessions_served(server, scene_id, desc, n_sessions=8, frames=120, width=1600, height=900, max_depth=12, warmup=3,
                         stream=None):
-    """Real-time SVGF sessions as a request class of `server` (pt_server_open_session): each session,
+    """Real-time SVGF sessions served by `server`'s session lane (pt_server_open_session): each session,
     on its own host thread, submits the frames of an orbit of the scene one after the other (frame
     k + 1 once frame k has been fetched). With `stream`, that request stream is served at the same time
     (run_served) and its summary returned beside the sessions'. Frame latency = server-side done time -
