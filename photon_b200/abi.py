@@ -161,7 +161,7 @@ class Tuning(C.Structure):
                 ("sort_by_material", C.c_int32), ("graph_bounces", C.c_int32), ("sort_rays", C.c_int32),
                 ("packed", C.c_int32), ("tail_paths", C.c_int32), ("wide_shadows", C.c_int32),
                 ("trace_refill", C.c_int32), ("shadow_refill", C.c_int32), ("walk_burst", C.c_int32),
-                ("sort_shadows", C.c_int32)]
+                ("sort_shadows", C.c_int32), ("pair_walk", C.c_int32)]
 
 
 class KernelTime(C.Structure):

@@ -203,10 +203,10 @@ struct Walker {
         }
         if (leaf_mode) {
             int i = ti;
-            const float4* g = ws.tris + kTriStride * i;  // 64-byte records: two 256-bit loads
-            float4 g0, g1, g2, g3;
+            const float4* g = ws.tris + kTriStride * i;  // 64-byte records: a 256-bit and a 128-bit load
+            float4 g0, g1;
             ldg_pair(g, g0, g1);
-            ldg_pair(g + 2, g2, g3);
+            const float4 g2 = __ldg(g + 2);  // the record's fourth float4 is padding
             float t, tu, tv;
             if (Count) cnt->tris++;
             if (tri_intersect(g0, g1, g2, o, d, tmax, t, tu, tv) &&
@@ -245,6 +245,112 @@ struct Walker {
                 --sp;
                 node = sp < kSmemStack ? stack[sp * stride] : overflow[sp - kSmemStack];
             }
+        }
+        return node >= 0;
+    }
+};
+
+// The ray of box_entry with its x and y halves in pairs and z alone: the same operations as
+// box_entry2 without the idle second half of the z pairs (two registers fewer per ray).
+struct RaySlab {
+    f32x2 oxy, ixy;
+    float oz, iz;
+};
+PT_HD RaySlab ray_slab(V3 o, V3 inv_d) { return {pack2(o.x, o.y), pack2(inv_d.x, inv_d.y), o.z, inv_d.z}; }
+PT_HD float box_entry3(float4 bmin, float4 bmax, const RaySlab& r, float tmax) {
+    float tx0, ty0, tx1, ty1;
+    unpack2(mul2(sub2(pack2(bmin.x, bmin.y), r.oxy), r.ixy), tx0, ty0);
+    unpack2(mul2(sub2(pack2(bmax.x, bmax.y), r.oxy), r.ixy), tx1, ty1);
+    const float tz0 = (bmin.z - r.oz) * r.iz, tz1 = (bmax.z - r.oz) * r.iz;
+    float tnear = fmax3(fminf(tx0, tx1), fminf(ty0, ty1), fmaxf(fminf(tz0, tz1), 0.0f));
+    float tfar = fmin3(fmaxf(tx0, tx1), fmaxf(ty0, ty1), fminf(fmaxf(tz0, tz1), tmax));
+    return tnear <= tfar ? tnear : kInf;
+}
+
+// Photon's traversal split for the pair walk: visit() is the node half of Walker::step (both child
+// slabs against tmax, the inner children ordered nearest first with side 0 first on a tie), and it
+// returns the triangles of the node's leaf children instead of testing them; the warp then tests
+// those (ray, triangle) pairs of all its lanes together (pair_pass in the walk kernels), which lowers
+// tmax to the nearest accepted triangle of the node's leaves exactly as the in-place tests would, and
+// decide() pushes the farther inner child, descends or pops with that tmax. So each ray's node visits
+// and its hit are Walker's.
+template <bool AnyHit, bool Count>
+struct PairWalker {
+    RaySlab rs;      // origin and inverse direction (the origin is rs.oxy, rs.oz)
+    V3 d;
+    float tmax;
+    int node;        // the node to visit next; -1 once the ray is finished
+    int sp;
+    int near, far;   // inner children of the last visit (-1: none), nearest first
+    float tn_near, tn_far;
+    int l0, n0, l1;  // leaf children of the last visit in side order: the first's triangles [l0, l0 + n0),
+                     // then the second's from l1 (their total is what visit() returned)
+    int tri;         // closest (or first accepted) triangle, -1 for none; its distance is tmax
+    float u, v;
+
+    PT_HD void init(V3 o_, V3 d_, float tmax_) {
+        d = d_;
+        rs = ray_slab(o_, V3{safe_inv(d_.x), safe_inv(d_.y), safe_inv(d_.z)});
+        tmax = tmax_;
+        node = 0;
+        sp = 0;
+        near = far = -1;
+        tn_near = tn_far = 0.0f;
+        l0 = n0 = l1 = 0;
+        tri = -1;
+        u = v = 0.0f;
+    }
+    PT_HD V3 origin() const {
+        float x, y;
+        unpack2(rs.oxy, x, y);
+        return V3{x, y, rs.oz};
+    }
+    // Visits `node`; returns how many triangles its leaf children hold (0: none).
+    PT_HD uint32_t visit(const float4* nodes, TraversalCounters* cnt) {
+        const float4* n = nodes + 4 * node;
+        float4 n0_, n1_, n2_, n3_;
+        ldg_pair(n, n0_, n1_);
+        ldg_pair(n + 2, n2_, n3_);
+        if (Count) cnt->nodes++;
+        const float tl = box_entry3(n0_, n1_, rs, tmax), tr = box_entry3(n2_, n3_, rs, tmax);
+        const int c0 = __float_as_int(n1_.w), i0 = __float_as_int(n0_.w), c1 = __float_as_int(n3_.w), i1 = __float_as_int(n2_.w);
+        const bool h0 = tl != kInf, h1 = tr != kInf;
+        const bool leaf0 = h0 && c0 > 0, leaf1 = h1 && c1 > 0;
+        const bool in0 = h0 && c0 <= 0 && i0 >= 0, in1 = h1 && c1 <= 0 && i1 >= 0;
+        near = in0 ? i0 : (in1 ? i1 : -1);
+        tn_near = in0 ? tl : tr;
+        far = (in0 && in1) ? i1 : -1;
+        tn_far = tr;
+        if (far >= 0 && tn_near > tn_far) {
+            const int a = near;
+            near = far;
+            far = a;
+            const float b = tn_near;
+            tn_near = tn_far;
+            tn_far = b;
+        }
+        l0 = leaf0 ? i0 : i1;
+        n0 = leaf0 ? c0 : (leaf1 ? c1 : 0);
+        l1 = i1;
+        return uint32_t(n0) + uint32_t(leaf0 && leaf1 ? c1 : 0);
+    }
+    // The triangle of the j-th pair of the last visit.
+    PT_HD int pair_triangle(uint32_t j) const { return int(j) < n0 ? l0 + int(j) : l1 + (int(j) - n0); }
+    // After the leaf tests: push the farther inner child, descend to the nearer or pop (traverse.h
+    // order); returns whether the ray goes on.
+    PT_HD bool decide(int* stack, int stride, int* overflow) {
+        if (far >= 0 && tn_far < tmax && sp < kStackSize) {
+            if (sp < kSmemStack) stack[sp * stride] = far;
+            else overflow[sp - kSmemStack] = far;
+            sp++;
+        }
+        if (near >= 0 && tn_near < tmax) {
+            node = near;
+        } else if (sp == 0) {
+            node = -1;
+        } else {
+            --sp;
+            node = sp < kSmemStack ? stack[sp * stride] : overflow[sp - kSmemStack];
         }
         return node >= 0;
     }
@@ -356,9 +462,9 @@ struct AnyWalker4 {
         if (leaf_mode) {
             const int i = ti;
             const float4* g = ws.tris + kTriStride * i;
-            float4 g0, g1, g2, g3;
+            float4 g0, g1;
             ldg_pair(g, g0, g1);
-            ldg_pair(g + 2, g2, g3);
+            const float4 g2 = __ldg(g + 2);  // the record's fourth float4 is padding
             float t, tu, tv;
             if (Count) cnt->tris++;
             if (tri_intersect(g0, g1, g2, o, d, tmax, t, tu, tv) &&

@@ -179,6 +179,7 @@ WfParams WavefrontEngine::params(const DevScene* scenes, int single, const DevVi
     p.trace_refill = uint32_t(std::clamp(tuning_.trace_refill, 1, 32));
     p.shadow_refill = uint32_t(std::clamp(tuning_.shadow_refill, 1, 32));
     p.walk_burst = uint32_t(std::clamp(tuning_.walk_burst, 1, 1 << 20));
+    p.pair_visits = uint32_t(std::clamp(tuning_.pair_walk, 0, 64));
     p.keys = keys_.ptr;
     p.hist = hist_.ptr;
     p.offsets = offsets_.ptr;
@@ -284,6 +285,7 @@ void WavefrontEngine::update_scheduling(const Tuning& t) {
     tuning_.trace_refill = t.trace_refill;
     tuning_.shadow_refill = t.shadow_refill;
     tuning_.walk_burst = t.walk_burst;
+    tuning_.pair_walk = t.pair_walk;
     const WfParams fresh = params(cont_params_.scenes, cont_params_.single_scene, cont_params_.views, cont_params_.num_views, false);
     cont_params_.sort_material = fresh.sort_material;
     cont_params_.packed = fresh.packed;
@@ -291,6 +293,7 @@ void WavefrontEngine::update_scheduling(const Tuning& t) {
     cont_params_.trace_refill = fresh.trace_refill;
     cont_params_.shadow_refill = fresh.shadow_refill;
     cont_params_.walk_burst = fresh.walk_burst;
+    cont_params_.pair_visits = fresh.pair_visits;
     if (cont_params_.sort_bits > 0) cont_params_.sort_bits = tuning_.sort_rays;
 }
 
@@ -748,6 +751,10 @@ void Renderer::set_tuning(const pt_tuning& t) {
         if (t.sort_shadows > 6) throw Error{PT_ERR_INVALID, "sort_shadows must be in [0, 6]"};
         cur.sort_shadows = t.sort_shadows;
     }
+    if (t.pair_walk >= 0) {
+        if (t.pair_walk > 64) throw Error{PT_ERR_INVALID, "pair_walk must be in [0, 64]"};
+        cur.pair_walk = t.pair_walk;
+    }
     engine_->set_tuning(cur);
 }
 
@@ -766,6 +773,7 @@ void Renderer::get_tuning(pt_tuning* t) const {
     t->shadow_refill = c.shadow_refill;
     t->walk_burst = c.walk_burst;
     t->sort_shadows = c.sort_shadows;
+    t->pair_walk = c.pair_walk;
 }
 
 // Coordinate descent over the knobs, one at a time, each candidate timed on the same probe view set.

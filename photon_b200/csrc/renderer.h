@@ -39,6 +39,8 @@ struct Tuning {
     int trace_refill = 24;         // a closest-hit warp claims new rays once fewer than this many lanes hold one
     int shadow_refill = 24;        // the same for the shadow walk
     int walk_burst = 16;           // walk steps a lane takes between two refill checks of its warp
+    int pair_walk = 0;             // > 0: pair walks (leaf triangles of a warp tested together) with up to
+                                   // this many node visits per warp step; 0: per-lane walks
     int sort_shadows = 0;          // origin bits per axis of the shadow-queue walk order (0: queue order);
                                    // iterations of at least 2M paths only. Off: on the 262K scene's 1080p
                                    // frame the shadow walk took 13.65 ms sorted against 13.63 unsorted (the

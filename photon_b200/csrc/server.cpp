@@ -651,6 +651,8 @@ void Server::set_tuning(const pt_tuning& t) {
     if (t.trace_refill > 0) cur.trace_refill = t.trace_refill;
     if (t.shadow_refill > 0) cur.shadow_refill = t.shadow_refill;
     if (t.walk_burst > 0) cur.walk_burst = t.walk_burst;
+    if (t.pair_walk > 64) throw Error{PT_ERR_INVALID, "pair_walk must be in [0, 64]"};
+    if (t.pair_walk >= 0) cur.pair_walk = t.pair_walk;
     pending_tuning_ = cur;  // (the shadow-queue order is not taken: the server's wavefront has no buffers for it)
     tuning_pending_ = true;
     cv_work_.notify_all();

@@ -237,6 +237,148 @@ __device__ __forceinline__ void walk_queue(uint32_t n, uint32_t* claim, uint32_t
     }
 }
 
+// ---- the pair walk -----------------------------------------------------------------------------------
+// A warp's shared memory in the pair walk (512 bytes after the block's stacks): the owners' result
+// slots. (The owners' rays reach the testing lanes by shuffles: shared memory taken here is L1 cache
+// lost to the node and triangle reads.)
+struct PairSlots {
+    unsigned long long best[32];  // nearest accepted pair: distance bits << 32 | pair (any-hit: pair); ~0 none
+    float2 uv[32];                // barycentrics of the pair a lane accepted
+};
+static_assert(sizeof(PairSlots) == 512, "PairSlots layout");
+
+// Tests the leaf pairs of a warp's lanes. Lane k, whose last node visit found m_k leaf triangles, owns
+// pairs [first_k, first_k + m_k) of the warp's list (an exclusive scan of m). The lanes take the list
+// 32 pairs at a time: lane j finds the owner of pair base + j by a binary search of the inclusive scan,
+// takes its ray and leaf ranges by shuffles (`scene`: the lane's own scene, in multi-scene launches),
+// tests that triangle against the owner's tmax, and an accepted pair enters the owner's slot by a
+// 64-bit atomicMin of (distance bits << 32 | pair index): positive distances order as their bits, so
+// the owner gets its least distance, on a tie its earliest pair. A sequential leaf walk (traverse.h
+// :93-104) accepts a triangle only when it lowers tmax, so it ends on the first pair of least distance
+// below the entering tmax: the same triangle, distance and barycentrics. Any-hit keys are the pair
+// index alone (the first accepted pair, where the sequential walk stops). An owner whose pairs span two
+// rounds enters the second with its lowered tmax (an answered any-hit ray with 0, which accepts
+// nothing).
+template <bool AnyHit, bool Count, bool Single, typename W>
+__device__ __forceinline__ void pair_pass(W& w, uint32_t m, PairSlots& ps, const WalkScene& uniform, const DevScene* scene,
+                                          TraversalCounters& tc) {
+    const uint32_t lane = lane_id();
+    uint32_t incl = m;
+#pragma unroll
+    for (uint32_t s = 1; s < 32; s <<= 1) {
+        const uint32_t x = __shfl_up_sync(kFull, incl, s);
+        if (lane >= s) incl += x;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31), first = incl - m;
+    const V3 o = w.origin();
+    float tmax = w.tmax;
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t p = base + lane;
+        uint32_t k = 0;
+#pragma unroll
+        for (uint32_t s = 16; s >= 1; s >>= 1) {
+            if (__shfl_sync(kFull, incl, k + s - 1) <= p) k += s;
+        }
+        const V3 ko{__shfl_sync(kFull, o.x, k), __shfl_sync(kFull, o.y, k), __shfl_sync(kFull, o.z, k)};
+        const V3 kd{__shfl_sync(kFull, w.d.x, k), __shfl_sync(kFull, w.d.y, k), __shfl_sync(kFull, w.d.z, k)};
+        const float kt = __shfl_sync(kFull, tmax, k);
+        const int j = int(p - __shfl_sync(kFull, first, k));
+        const int kn0 = __shfl_sync(kFull, w.n0, k), kl0 = __shfl_sync(kFull, w.l0, k), kl1 = __shfl_sync(kFull, w.l1, k);
+        const DevScene* sc = Single ? uniform.scene : reinterpret_cast<const DevScene*>(__shfl_sync(kFull, reinterpret_cast<unsigned long long>(scene), k));
+        if (p < total) {
+            const int i = j < kn0 ? kl0 + j : kl1 + (j - kn0);
+            const float4* g = (Single ? uniform.tris : sc->tris) + kTriStride * i;
+            float4 g0, g1;
+            ldg_pair(g, g0, g1);
+            const float4 g2 = __ldg(g + 2);  // the record's fourth float4 is padding
+            float t, tu, tv;
+            if (Count) tc.tris++;
+            if (tri_intersect(g0, g1, g2, ko, kd, kt, t, tu, tv) &&
+                !((__float_as_int(g1.w) & 1) && alpha_passes(*sc, i, __float_as_int(g0.w), tu, tv))) {
+                const unsigned long long key = AnyHit ? (unsigned long long)p : ((unsigned long long)__float_as_uint(t) << 32 | p);
+                atomicMin(&ps.best[k], key);
+                if (!AnyHit) ps.uv[lane] = make_float2(tu, tv);
+            }
+        }
+        __syncwarp();
+        if (m) {
+            const unsigned long long key = ps.best[lane];
+            if (key != ~0ull) {
+                ps.best[lane] = ~0ull;
+                const uint32_t pw = uint32_t(key);
+                w.tri = w.pair_triangle(pw - first);
+                if (!AnyHit) {
+                    w.tmax = __uint_as_float(uint32_t(key >> 32));
+                    const float2 uv = ps.uv[pw - base];
+                    w.u = uv.x;
+                    w.v = uv.y;
+                }
+                tmax = AnyHit ? 0.0f : w.tmax;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Persistent walk over a ray queue in warp steps of the pair walk: in each of `visits` rounds, every
+// live lane that has not yet met leaf children visits its next node; then the warp tests all the leaf
+// pairs met together (pair_pass) and their owners decide. Every lane is at a node at the start of a
+// step, so the node visits run on all live lanes at once, and a leaf's triangles are tested by as many
+// lanes as it has triangles, instead of the triangle tests of a few lanes running beside the node
+// visits of the others. (A warp-wide vote in the rounds, to end them once enough lanes wait, measured
+// slower: the rounds then reconverge the warp after every visit.) Refill, begin and end as in
+// walk_queue, checked once per step. Count: tc.steps counts node visits and warp_steps the rounds.
+template <typename W, int Overflow, bool AnyHit, bool Count, bool Single, typename Begin, typename End>
+__device__ __forceinline__ void walk_queue_pairs(uint32_t n, uint32_t* claim, uint32_t refill, uint32_t visits, int* stack, int stride,
+                                                 PairSlots& ps, const WalkScene& uniform, TraversalCounters& tc, uint32_t& warp_steps,
+                                                 Begin begin, End end) {
+    int overflow[Overflow];
+    W w;
+    WalkScene ws = uniform;
+    uint32_t idx = 0;
+    bool live = false, drained = false;
+    const uint32_t lane = lane_id(), below = (1u << lane) - 1u;
+    ps.best[lane] = ~0ull;
+    for (;;) {
+        uint32_t act = __ballot_sync(kFull, live);
+        if (!drained && uint32_t(__popc(act)) < refill) {
+            const uint32_t idle = ~act, want = uint32_t(__popc(idle));
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(claim, want);
+            base = __shfl_sync(kFull, base, 0);
+            drained = base + want >= n;
+            if (!live) {
+                const uint32_t r = base + uint32_t(__popc(idle & below));
+                if (r < n) {
+                    idx = begin(r, w, ws);
+                    live = true;
+                }
+            }
+            act = __ballot_sync(kFull, live);
+        }
+        if (act == 0) break;
+        uint32_t m = 0;
+        for (uint32_t it = 0; it < visits; it++) {
+            if (live && m == 0) {
+                m = w.visit(Single ? uniform.nodes : ws.nodes, &tc);
+                if (Count) tc.steps++;
+                if (m == 0 && !w.decide(stack, stride, overflow)) {
+                    end(idx, w);
+                    live = false;
+                }
+            }
+            if (Count) warp_steps++;
+        }
+        if (__any_sync(kFull, m != 0)) {
+            pair_pass<AnyHit, Count, Single>(w, m, ps, uniform, ws.scene, tc);
+            if (m && ((AnyHit && w.tri >= 0) || !w.decide(stack, stride, overflow))) {
+                end(idx, w);
+                live = false;
+            }
+        }
+    }
+}
+
 // The scene arrays of a launch whose views all use one scene (the renderer), or null arrays (the
 // server: each ray's scene comes from its view).
 __device__ __forceinline__ WalkScene single_walk_scene(const WfParams& P, bool wide) {
@@ -281,6 +423,42 @@ __global__ void __maxnreg__(56) k_trace(const __grid_constant__ WfParams P) {
             },
             end);
     }
+    if (Count) {
+        warp_add_u64(&c->node_visits, tc.nodes);
+        warp_add_u64(&c->tri_tests, tc.tris);
+        warp_add_u64(&c->trace_lane_steps, tc.steps);
+        if (lane_id() == 0) atomicAdd(&c->trace_warp_steps, (unsigned long long)warp_steps);
+    }
+}
+
+// The closest-hit walk as a pair walk (walk_queue_pairs): the same hits as k_trace. Dynamic shared
+// memory: the stacks, then one PairSlots per warp.
+template <bool Count, bool Single>
+__global__ void __maxnreg__(56) k_trace_pairs(const __grid_constant__ WfParams P) {
+    extern __shared__ int smem_stack[];
+    int* stack = smem_stack + threadIdx.x;
+    PairSlots& ps = reinterpret_cast<PairSlots*>(smem_stack + kSmemStack * blockDim.x)[threadIdx.x >> 5];
+    Counters* c = P.ctr;
+    if (c->tail) return;
+    const uint32_t p = c->parity, n = c->count[p];
+    TraversalCounters tc{0, 0, 0};
+    uint32_t warp_steps = 0;
+    using W = PairWalker<false, Count>;
+    auto end = [&](uint32_t i, const W& w) {
+        P.pb.hit[i] = w.tri >= 0 ? make_float4(w.tmax, __int_as_float(w.tri), w.u, w.v) : make_float4(kInf, __int_as_float(-1), 0.0f, 0.0f);
+    };
+    const WalkScene uni = single_walk_scene(P, false);
+    walk_queue_pairs<W, kStackSize - kSmemStack, false, Count, Single>(
+        n, &c->fetch[1], P.trace_refill, P.pair_visits, stack, blockDim.x, ps, uni, tc, warp_steps,
+        [&](uint32_t i, W& w, WalkScene& ws) {
+            if (!Single) {
+                const DevScene& s = P.scenes[P.views[P.pb.id[p][i].x].scene];
+                ws = WalkScene{s.nodes, s.tris, &s};
+            }
+            w.init(xyz(P.pb.o[p][i]), xyz(P.pb.d[p][i]), kInf);
+            return i;
+        },
+        end);
     if (Count) {
         warp_add_u64(&c->node_visits, tc.nodes);
         warp_add_u64(&c->tri_tests, tc.tris);
@@ -658,20 +836,27 @@ __global__ void __launch_bounds__(256) k_tail(const __grid_constant__ WfParams P
 // resident warps than it loses to the tighter allocation (measured; the closest-hit walk does not).
 // Wide: the 4-wide BVH, used when every ray of the launch has it (a single scene that carries one);
 // otherwise the BVH2.
-template <bool Count, bool Packed, bool Wide, bool Single>
-__global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfParams P) {
-    extern __shared__ int smem_stack[];
-    int* stack = smem_stack + threadIdx.x;
-    Counters* c = P.ctr;
-    if (c->tail) return;
-    const uint32_t q = c->parity ^ 1u, n = c->shadow_count;
-    TraversalCounters tc{0, 0, 0};
-    uint32_t warp_steps = 0;
+// The shadow queue of an iteration: the order it is walked in, and the delivery of unoccluded rays.
+struct ShadowQueue {
+    const WfParams& P;
+    uint32_t q;   // parity of the paths the rays contribute to
+    bool sorted;
     // Queue position -> record: the sorted order of this iteration's shadow rays, or the queue's own.
-    const bool sorted = c->shadow_sorting != 0;
-    auto record = [&](uint32_t i) { return sorted ? __ldg(P.shadow_perm + i) : i; };
+    __device__ __forceinline__ uint32_t record(uint32_t i) const { return sorted ? __ldg(P.shadow_perm + i) : i; }
+    // Starts walker w on queue position i; returns the record.
+    template <typename W>
+    __device__ __forceinline__ uint32_t init(uint32_t i, W& w) const {
+        const uint32_t j = record(i);
+        const float4 a = P.pb.sh0[j];
+        w.init(xyz(a), xyz(P.pb.sh1[j]), a.w);
+        return j;
+    }
+    // The scene of record j (multi-scene launches).
+    __device__ __forceinline__ const DevScene& scene(uint32_t j) const {
+        return P.scenes[P.views[__float_as_uint(P.pb.sh2[j].w) & 0x7fffffffu].scene];
+    }
     // An unoccluded shadow ray adds its contribution to its path (or to its finished sample).
-    auto deliver = [&](uint32_t i) {
+    __device__ __forceinline__ void deliver(uint32_t i) const {
         const float4 cc = P.pb.sh2[i];
         const uint32_t tag = __float_as_uint(cc.w), view = tag & 0x7fffffffu, target = __float_as_uint(P.pb.sh1[i].w);
         if (tag & 0x80000000u) {
@@ -686,13 +871,21 @@ __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfPar
             P.pb.beta[q][target] = b4;
             P.pb.lr[q][target] = l4;
         }
-    };
-    auto init = [&](uint32_t i, auto& w) {
-        const uint32_t j = record(i);
-        const float4 a = P.pb.sh0[j];
-        w.init(xyz(a), xyz(P.pb.sh1[j]), a.w);
-        return j;
-    };
+    }
+};
+
+template <bool Count, bool Packed, bool Wide, bool Single>
+__global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfParams P) {
+    extern __shared__ int smem_stack[];
+    int* stack = smem_stack + threadIdx.x;
+    Counters* c = P.ctr;
+    if (c->tail) return;
+    const uint32_t n = c->shadow_count;
+    TraversalCounters tc{0, 0, 0};
+    uint32_t warp_steps = 0;
+    const ShadowQueue sq{P, c->parity ^ 1u, c->shadow_sorting != 0};
+    auto deliver = [&](uint32_t i) { sq.deliver(i); };
+    auto init = [&](uint32_t i, auto& w) { return sq.init(i, w); };
     if (Wide && Single && P.scenes[P.single_scene].nodes4) {
         using W4 = AnyWalker4<Count, Packed>;
         walk_queue<W4, kBvh4Stack - kSmemStack, Count, true>(
@@ -714,13 +907,47 @@ __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfPar
                 n, &c->fetch[3], P.shadow_refill, P.walk_burst, stack, blockDim.x, WalkScene{nullptr, nullptr, nullptr}, tc, warp_steps,
                 [&](uint32_t i, W& w, WalkScene& ws) {
                     const uint32_t j = init(i, w);
-                    const DevScene& s = P.scenes[P.views[__float_as_uint(P.pb.sh2[j].w) & 0x7fffffffu].scene];
+                    const DevScene& s = sq.scene(j);
                     ws = WalkScene{s.nodes, s.tris, &s};
                     return j;
                 },
                 end);
         }
     }
+    if (Count) {
+        warp_add_u64(&c->shadow_node_visits, tc.nodes);
+        warp_add_u64(&c->shadow_tri_tests, tc.tris);
+        warp_add_u64(&c->shadow_lane_steps, tc.steps);
+        if (lane_id() == 0) atomicAdd(&c->shadow_warp_steps, (unsigned long long)warp_steps);
+    }
+}
+
+// The any-hit walk as a pair walk (walk_queue_pairs) over the BVH2: the same answers as k_shadow.
+template <bool Count, bool Single>
+__global__ void __maxnreg__(56) k_shadow_pairs(const __grid_constant__ WfParams P) {
+    extern __shared__ int smem_stack[];
+    int* stack = smem_stack + threadIdx.x;
+    PairSlots& ps = reinterpret_cast<PairSlots*>(smem_stack + kSmemStack * blockDim.x)[threadIdx.x >> 5];
+    Counters* c = P.ctr;
+    if (c->tail) return;
+    const uint32_t n = c->shadow_count;
+    TraversalCounters tc{0, 0, 0};
+    uint32_t warp_steps = 0;
+    const ShadowQueue sq{P, c->parity ^ 1u, c->shadow_sorting != 0};
+    using W = PairWalker<true, Count>;
+    walk_queue_pairs<W, kStackSize - kSmemStack, true, Count, Single>(
+        n, &c->fetch[3], P.shadow_refill, P.pair_visits, stack, blockDim.x, ps, single_walk_scene(P, false), tc, warp_steps,
+        [&](uint32_t i, W& w, WalkScene& ws) {
+            const uint32_t j = sq.init(i, w);
+            if (!Single) {
+                const DevScene& s = sq.scene(j);
+                ws = WalkScene{s.nodes, s.tris, &s};
+            }
+            return j;
+        },
+        [&](uint32_t i, const W& w) {
+            if (w.tri < 0) sq.deliver(i);
+        });
     if (Count) {
         warp_add_u64(&c->shadow_node_visits, tc.nodes);
         warp_add_u64(&c->shadow_tri_tests, tc.tris);
@@ -1052,6 +1279,21 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
     }
+    const size_t pair_smem = smem + size_t(trace_block / 32) * sizeof(PairSlots);
+    const void* pair_kernels[] = {(const void*)k_trace_pairs<false, false>, (const void*)k_trace_pairs<false, true>,
+                                  (const void*)k_trace_pairs<true, false>,  (const void*)k_trace_pairs<true, true>,
+                                  (const void*)k_shadow_pairs<false, false>, (const void*)k_shadow_pairs<false, true>,
+                                  (const void*)k_shadow_pairs<true, false>,  (const void*)k_shadow_pairs<true, true>};
+    for (const void* k : pair_kernels) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pair_smem));
+        if (e != cudaSuccess) return e;
+    }
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace_pairs<false, false>, trace_block, pair_smem);
+    if (e != cudaSuccess) return e;
+    out->pair_trace_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shadow_pairs<false, false>, trace_block, pair_smem);
+    if (e != cudaSuccess) return e;
+    out->pair_shadow_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
     // Grids are sized for the heavier (multi-scene) variants, so that every variant's grid fits.
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace<false, true, false>, trace_block, smem);
     if (e != cudaSuccess) return e;
@@ -1069,6 +1311,12 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
 
 template <bool Count, bool Packed, bool Single>
 static void launch_traversals(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, size_t smem, bool shadow) {
+    if (Packed && p.pair_visits > 0 && !(shadow && p.wide_shadows)) {
+        const size_t pair_smem = smem + size_t(ls.trace_block / 32) * sizeof(PairSlots);
+        if (shadow) k_shadow_pairs<Count, Single><<<ls.pair_shadow_grid, ls.shadow_block, pair_smem, stream>>>(p);
+        else k_trace_pairs<Count, Single><<<ls.pair_trace_grid, ls.trace_block, pair_smem, stream>>>(p);
+        return;
+    }
     if (shadow) {
         if (p.wide_shadows) k_shadow<Count, Packed, true, Single><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);
         else k_shadow<Count, Packed, false, Single><<<ls.shadow_grid, ls.shadow_block, smem, stream>>>(p);

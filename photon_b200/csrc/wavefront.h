@@ -91,6 +91,8 @@ struct WfParams {
     uint32_t trace_refill;     // 1-32: a trace warp claims new rays once fewer of its lanes hold one
     uint32_t shadow_refill;    // the same for the shadow walk
     uint32_t walk_burst;       // walk steps each lane takes between two looks at its warp (>= 1)
+    uint32_t pair_visits;      // > 0: the BVH2 walks are pair walks with up to this many node visits per
+                               //      warp step (packed slab tests only); 0: per-lane walks
     int sort_material;         // 1: the shade kernel groups each block's paths by material class
     int sort_bits;             // > 0: sort continuing paths by direction octant + Morton origin cell
                                //      (this many bits per axis) before they are traced
@@ -115,6 +117,7 @@ struct LaunchShape {
     int trace_grid, trace_block;
     int shade_grid, shade_block;
     int shadow_grid, shadow_block;
+    int pair_trace_grid, pair_shadow_grid;  // the pair walks (more shared memory per block)
 };
 
 // Fills grid sizes from the occupancy of each kernel on `device` (block sizes as requested).

@@ -254,7 +254,7 @@ class Renderer:
         return p
 
     def set_tuning(self, **kw):
-        t = abi.Tuning(0, 0, 0, -1, -1, -1, -1, -1, -1, 0, 0, 0, -1)
+        t = abi.Tuning(0, 0, 0, -1, -1, -1, -1, -1, -1, 0, 0, 0, -1, -1)
         for k, v in kw.items():
             setattr(t, k, v)
         _check(lib.pt_set_tuning(self.h, C.byref(t)), self._err)
@@ -459,7 +459,7 @@ class Server:
 
     def set_tuning(self, **kw):
         """Applies tuning knobs (pt_server_set_tuning); unnamed knobs keep their values."""
-        t = abi.Tuning(0, 0, 0, -1, -1, -1, -1, -1, -1, 0, 0, 0, -1)
+        t = abi.Tuning(0, 0, 0, -1, -1, -1, -1, -1, -1, 0, 0, 0, -1, -1)
         for k, v in kw.items():
             setattr(t, k, v)
         _check(lib.pt_server_set_tuning(self.h, C.byref(t)), self._err)

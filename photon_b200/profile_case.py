@@ -21,6 +21,8 @@ def main(argv=None):
     ap.add_argument("--triangles", type=int, default=262144)
     ap.add_argument("--depth", type=int, default=12)
     ap.add_argument("--denoise", type=int, default=0, help="render this many real-time SVGF frames instead")
+    ap.add_argument("--tuning", action="append", default=[], metavar="KNOB=VALUE",
+                    help="a pt_tuning knob for the render (repeatable), e.g. --tuning pair_walk=6")
     a = ap.parse_args(argv)
     g = native.terrain_scene(a.triangles, 1)
     b = g.build()
@@ -29,7 +31,7 @@ def main(argv=None):
     r = native.Renderer(0)
     r.upload(b.desc)
     r.resize(a.width, a.height)
-    r.set_tuning(graph_bounces=0)
+    r.set_tuning(graph_bounces=0, **{k: int(v) for k, v in (t.split("=", 1) for t in a.tuning)})
     if a.denoise:
         from . import workloads
         cams = workloads.orbit_cameras(b.desc, a.denoise, a.width / a.height)
