@@ -262,9 +262,10 @@ typedef struct pt_tuning {
                                   2,097,152 paths ordered by direction octant + Morton origin cell (this
                                   many bits per axis); -1 keep */
     int32_t pair_walk;         /* 0: each lane walks its ray through node visits and triangle tests on its own;
-                                  1-64: pair walks, with the leaf triangles a warp's rays reach tested by all
-                                  its lanes together after up to this many node visits per lane (same hits
-                                  and answers; packed slab tests only); -1 keep */
+                                  1-64 (default 5): pair walks, with the leaf triangles a warp's rays reach
+                                  tested by all its lanes together after up to this many node visits per
+                                  lane (same hits and answers; packed slab tests and the BVH2 only, so
+                                  packed = 0 and the 4-wide shadow walk use the per-lane walks); -1 keep */
 } pt_tuning;
 int32_t pt_set_tuning(pt_renderer* r, const pt_tuning* t);
 int32_t pt_get_tuning(const pt_renderer* r, pt_tuning* t);

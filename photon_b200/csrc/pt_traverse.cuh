@@ -13,7 +13,7 @@
 namespace ptw {
 
 constexpr int kStackSize = 64;     // Photon's kStackSize (traverse.h:22)
-constexpr int kSmemStack = 24;     // entries per thread kept in shared memory
+constexpr int kSmemStack = 16;     // entries per thread kept in shared memory
 
 struct Hit {
     float t;
@@ -273,40 +273,46 @@ PT_HD float box_entry3(float4 bmin, float4 bmax, const RaySlab& r, float tmax) {
 // those (ray, triangle) pairs of all its lanes together (pair_pass in the walk kernels), which lowers
 // tmax to the nearest accepted triangle of the node's leaves exactly as the in-place tests would, and
 // decide() pushes the farther inner child, descends or pops with that tmax. So each ray's node visits
-// and its hit are Walker's.
+// and its hit are Walker's. What only the pair pass and the ray's end read (the direction, the leaf
+// ranges, the hit's triangle and barycentrics) lives in the lane's shared-memory slots, not in
+// registers: PairLane refers to them. (The inner children of a visit that waits for its leaf tests
+// stay in registers: parked in shared memory too, the walk measured slower.)
+struct PairLane {
+    float4& ray;    // direction, tmax as of the lane's last pair pass
+    int4& leaves;   // the last visit's leaf children in side order: first triangles and count of the
+                    // first ([l0, l0 + n0)), first triangle of the second, and the lane's first pair
+    float4& hit;    // closest (or first accepted) triangle (bits; -1: none), u, v
+};
+
+// The inner children of a visit (-1: none), nearest first, and their entry distances.
+struct NodeChoice {
+    int near, far;
+    float tn_near, tn_far;
+};
+
 template <bool AnyHit, bool Count>
 struct PairWalker {
     RaySlab rs;      // origin and inverse direction (the origin is rs.oxy, rs.oz)
-    V3 d;
     float tmax;
     int node;        // the node to visit next; -1 once the ray is finished
     int sp;
-    int near, far;   // inner children of the last visit (-1: none), nearest first
-    float tn_near, tn_far;
-    int l0, n0, l1;  // leaf children of the last visit in side order: the first's triangles [l0, l0 + n0),
-                     // then the second's from l1 (their total is what visit() returned)
-    int tri;         // closest (or first accepted) triangle, -1 for none; its distance is tmax
-    float u, v;
 
-    PT_HD void init(V3 o_, V3 d_, float tmax_) {
-        d = d_;
+    PT_HD void init(V3 o_, V3 d_, float tmax_, const PairLane& sl) {
         rs = ray_slab(o_, V3{safe_inv(d_.x), safe_inv(d_.y), safe_inv(d_.z)});
         tmax = tmax_;
         node = 0;
         sp = 0;
-        near = far = -1;
-        tn_near = tn_far = 0.0f;
-        l0 = n0 = l1 = 0;
-        tri = -1;
-        u = v = 0.0f;
+        sl.ray = make_float4(d_.x, d_.y, d_.z, tmax_);
+        sl.hit = make_float4(__int_as_float(-1), 0.0f, 0.0f, 0.0f);
     }
     PT_HD V3 origin() const {
         float x, y;
         unpack2(rs.oxy, x, y);
         return V3{x, y, rs.oz};
     }
-    // Visits `node`; returns how many triangles its leaf children hold (0: none).
-    PT_HD uint32_t visit(const float4* nodes, TraversalCounters* cnt) {
+    // Visits `node`: its inner children into `ch`; returns how many triangles its leaf children hold
+    // (0: none), whose ranges it leaves in the lane's slot.
+    PT_HD uint32_t visit(const float4* nodes, const PairLane& sl, NodeChoice& ch, TraversalCounters* cnt) {
         const float4* n = nodes + 4 * node;
         float4 n0_, n1_, n2_, n3_;
         ldg_pair(n, n0_, n1_);
@@ -317,35 +323,33 @@ struct PairWalker {
         const bool h0 = tl != kInf, h1 = tr != kInf;
         const bool leaf0 = h0 && c0 > 0, leaf1 = h1 && c1 > 0;
         const bool in0 = h0 && c0 <= 0 && i0 >= 0, in1 = h1 && c1 <= 0 && i1 >= 0;
-        near = in0 ? i0 : (in1 ? i1 : -1);
-        tn_near = in0 ? tl : tr;
-        far = (in0 && in1) ? i1 : -1;
-        tn_far = tr;
-        if (far >= 0 && tn_near > tn_far) {
-            const int a = near;
-            near = far;
-            far = a;
-            const float b = tn_near;
-            tn_near = tn_far;
-            tn_far = b;
+        ch.near = in0 ? i0 : (in1 ? i1 : -1);
+        ch.tn_near = in0 ? tl : tr;
+        ch.far = (in0 && in1) ? i1 : -1;
+        ch.tn_far = tr;
+        if (ch.far >= 0 && ch.tn_near > ch.tn_far) {
+            const int a = ch.near;
+            ch.near = ch.far;
+            ch.far = a;
+            const float b = ch.tn_near;
+            ch.tn_near = ch.tn_far;
+            ch.tn_far = b;
         }
-        l0 = leaf0 ? i0 : i1;
-        n0 = leaf0 ? c0 : (leaf1 ? c1 : 0);
-        l1 = i1;
-        return uint32_t(n0) + uint32_t(leaf0 && leaf1 ? c1 : 0);
+        if (!(leaf0 || leaf1)) return 0;
+        const int n0 = leaf0 ? c0 : c1, n1 = leaf0 && leaf1 ? c1 : 0;
+        sl.leaves = make_int4(leaf0 ? i0 : i1, n0, i1, 0);
+        return uint32_t(n0 + n1);
     }
-    // The triangle of the j-th pair of the last visit.
-    PT_HD int pair_triangle(uint32_t j) const { return int(j) < n0 ? l0 + int(j) : l1 + (int(j) - n0); }
     // After the leaf tests: push the farther inner child, descend to the nearer or pop (traverse.h
     // order); returns whether the ray goes on.
-    PT_HD bool decide(int* stack, int stride, int* overflow) {
-        if (far >= 0 && tn_far < tmax && sp < kStackSize) {
-            if (sp < kSmemStack) stack[sp * stride] = far;
-            else overflow[sp - kSmemStack] = far;
+    PT_HD bool decide(const NodeChoice& ch, int* stack, int stride, int* overflow) {
+        if (ch.far >= 0 && ch.tn_far < tmax && sp < kStackSize) {
+            if (sp < kSmemStack) stack[sp * stride] = ch.far;
+            else overflow[sp - kSmemStack] = ch.far;
             sp++;
         }
-        if (near >= 0 && tn_near < tmax) {
-            node = near;
+        if (ch.near >= 0 && ch.tn_near < tmax) {
+            node = ch.near;
         } else if (sp == 0) {
             node = -1;
         } else {
@@ -355,6 +359,9 @@ struct PairWalker {
         return node >= 0;
     }
 };
+
+// The triangle of pair j of a visit whose leaf ranges are lv (PairLane::leaves).
+PT_HD int pair_triangle(const int4& lv, int j) { return j < lv.y ? lv.x + j : lv.z + (j - lv.y); }
 
 // One ray's traversal: AnyHit stops at the first accepted triangle. `stack` is this thread's column of
 // the block's shared stack (entry k at stack[k * stride]).

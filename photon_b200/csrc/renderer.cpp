@@ -161,13 +161,20 @@ void WavefrontEngine::ensure_shape() {
     shape_ok_ = true;
 }
 
-WfParams WavefrontEngine::params(const DevScene* scenes, int single, const DevView* views, int n, bool count) const {
+WfParams WavefrontEngine::params(const DevScene* scenes, int single, const DevScene* single_host, const DevView* views, int n,
+                                 bool count) const {
     WfParams p;
     std::memset(&p, 0, sizeof(p));  // padding too: captured graphs are matched by comparing the bytes
     p.scenes = scenes;
     p.views = views;
     p.num_views = n;
     p.single_scene = single;
+    if (single >= 0) {
+        if (!single_host) throw Error{PT_ERR_INVALID, "a single-scene pass needs the scene's host copy"};
+        p.single_nodes = single_host->nodes;
+        p.single_nodes4 = single_host->nodes4;
+        p.single_tris = single_host->tris;
+    }
     p.pb = pb_;
     p.ctr = ctr_.ptr;
     p.count_work = count ? 1 : 0;
@@ -222,8 +229,8 @@ void WavefrontEngine::capture(const WfParams& p) {
     graph_iters_ = iters;
 }
 
-void WavefrontEngine::run(const DevScene* scenes, int single_scene, const DevView* views, int n_views, uint64_t total_work,
-                          bool count_work) {
+void WavefrontEngine::run(const DevScene* scenes, int single_scene, const DevScene* single, const DevView* views, int n_views,
+                          uint64_t total_work, bool count_work) {
     if (total_work == 0) return;
     cudaError_t stale = cudaGetLastError();
     if (stale != cudaSuccess) throw Error{PT_ERR_CUDA, std::string("an earlier CUDA call failed: ") + cudaGetErrorString(stale)};
@@ -235,7 +242,7 @@ void WavefrontEngine::run(const DevScene* scenes, int single_scene, const DevVie
     h_ctr_->work_total = total_work;
     h_ctr_->tail_limit = tail_limit(tuning_.tail_paths, busy.others == 0);
     PTW_CUDA(cudaMemcpyAsync(ctr_.ptr, h_ctr_, sizeof(Counters), cudaMemcpyHostToDevice, stream_));
-    WfParams p = params(scenes, single_scene, views, n_views, count_work || (profile_flags_ & PT_PROFILE_TRAVERSAL_COUNTS));
+    WfParams p = params(scenes, single_scene, single, views, n_views, count_work || (profile_flags_ & PT_PROFILE_TRAVERSAL_COUNTS));
     // A render too small for any iteration to reach the sorting threshold launches no sort kernels.
     if (std::min<uint64_t>(total_work, uint64_t(tuning_.path_capacity)) < kSortMinPaths) {
         p.sort_bits = 0;
@@ -272,7 +279,7 @@ void WavefrontEngine::begin(const DevScene* scenes, const DevView* views, int n_
     h_ctr_->tail_limit = tail_limit(tuning_.tail_paths, false);  // a server shares the GPU between requests
     tail_limit_ = h_ctr_->tail_limit;
     PTW_CUDA(cudaMemcpyAsync(ctr_.ptr, h_ctr_, sizeof(Counters), cudaMemcpyHostToDevice, stream_));
-    cont_params_ = params(scenes, -1, views, n_views, false);
+    cont_params_ = params(scenes, -1, nullptr, views, n_views, false);
 }
 
 void WavefrontEngine::update_scheduling(const Tuning& t) {
@@ -286,7 +293,7 @@ void WavefrontEngine::update_scheduling(const Tuning& t) {
     tuning_.shadow_refill = t.shadow_refill;
     tuning_.walk_burst = t.walk_burst;
     tuning_.pair_walk = t.pair_walk;
-    const WfParams fresh = params(cont_params_.scenes, cont_params_.single_scene, cont_params_.views, cont_params_.num_views, false);
+    const WfParams fresh = params(cont_params_.scenes, -1, nullptr, cont_params_.views, cont_params_.num_views, false);
     cont_params_.sort_material = fresh.sort_material;
     cont_params_.packed = fresh.packed;
     cont_params_.wide_shadows = fresh.wide_shadows;
@@ -491,7 +498,7 @@ void Renderer::render_pass_set(std::vector<DevView>& views, int /*spp_total*/, s
         }
         if (d_views_.count < table.size()) d_views_.allocate(table.size());
         PTW_CUDA(cudaMemcpyAsync(d_views_.ptr, table.data(), table.size() * sizeof(DevView), cudaMemcpyHostToDevice, stream_));
-        engine_->run(scene_.device_view(), 0, d_views_.ptr, int(table.size()), work);
+        engine_->run(scene_.device_view(), 0, &scene_.view(), d_views_.ptr, int(table.size()), work);
         last_ctr_ = engine_->last();
         profile_.closest_rays += last_ctr_.rays;
         profile_.shadow_rays += last_ctr_.shadow_rays;
@@ -835,6 +842,7 @@ void Renderer::tune_on(const std::vector<pt_view>& probe, pt_tuning* chosen, dou
         try_knob([](Tuning& t, int v) { t.shadow_refill = v; }, {1, 8, 16, 24, 32});
         try_knob([](Tuning& t, int v) { t.walk_burst = v; }, {4, 8, 16, 32, 64});
         try_knob([](Tuning& t, int v) { t.sort_shadows = v; }, {0, 3, 4, 5});
+        try_knob([](Tuning& t, int v) { t.pair_walk = v; }, {0, 3, 5, 8});
         engine_->set_tuning(best);
         if (tuned_rate) *tuned_rate = best_rate;
         if (chosen) get_tuning(chosen);

@@ -39,8 +39,10 @@ struct Tuning {
     int trace_refill = 24;         // a closest-hit warp claims new rays once fewer than this many lanes hold one
     int shadow_refill = 24;        // the same for the shadow walk
     int walk_burst = 16;           // walk steps a lane takes between two refill checks of its warp
-    int pair_walk = 0;             // > 0: pair walks (leaf triangles of a warp tested together) with up to
-                                   // this many node visits per warp step; 0: per-lane walks
+    int pair_walk = 5;             // > 0: pair walks (leaf triangles of a warp tested together) with up to
+                                   // this many node visits per warp step; 0: per-lane walks. On the 262K
+                                   // scene's 1080p frame: trace 28.2 -> 24.0 ms, shadow 13.7 -> 11.0 ms
+                                   // (4 to 6 visits within noise; 2: 26.1 ms, 10: 25.6 ms)
     int sort_shadows = 0;          // origin bits per axis of the shadow-queue walk order (0: queue order);
                                    // iterations of at least 2M paths only. Off: on the 262K scene's 1080p
                                    // frame the shadow walk took 13.65 ms sorted against 13.63 unsorted (the
@@ -64,9 +66,10 @@ public:
 
     // Renders one pass: every work item of `views` (device table of n views, work ranges
     // contiguous from 0) until all paths finished. scenes: device table; single_scene >= 0 when
-    // all views share that slot. Blocks the host until done (bounded by max_iterations).
-    void run(const DevScene* scenes, int single_scene, const DevView* views, int n_views, uint64_t total_work,
-             bool count_work = false);
+    // all views share that slot, whose host copy is `single` (its device array pointers). Blocks the
+    // host until done (bounded by max_iterations).
+    void run(const DevScene* scenes, int single_scene, const DevScene* single, const DevView* views, int n_views,
+             uint64_t total_work, bool count_work = false);
 
     // Continuous mode (the request server): prepare once, then alternate iterate() with host-side
     // admission of new work (append_work) and completion checks (counters()).
@@ -114,7 +117,7 @@ public:
 private:
     void ensure_shape();
     void capture(const WfParams& p);
-    WfParams params(const DevScene* scenes, int single, const DevView* views, int n, bool count) const;
+    WfParams params(const DevScene* scenes, int single, const DevScene* single_host, const DevView* views, int n, bool count) const;
 
     int device_;
     cudaStream_t stream_;

@@ -551,7 +551,8 @@ void Server::session_loop() {
                                      session_stream_));
             PTW_CUDA(cudaMemcpyAsync(session_views_.ptr, views.data(), views.size() * sizeof(DevView), cudaMemcpyHostToDevice,
                                      session_stream_));
-            session_engine_->run(session_scenes_.ptr, single, session_views_.ptr, int(views.size()), work);
+            session_engine_->run(session_scenes_.ptr, single, single >= 0 ? &table[size_t(single)] : nullptr, session_views_.ptr,
+                                 int(views.size()), work);
             for (size_t k = 0; k < frames.size(); k++) {
                 Request& r = *frames[k];
                 Session& ses = *r.ses;
@@ -817,6 +818,10 @@ void Server::loop() {
                 PTW_CUDA(cudaMemcpyAsync(d_views_.ptr + views_uploaded_, B.views, n_new * sizeof(DevView), cudaMemcpyHostToDevice, stream_));
                 views_uploaded_ = views_.size();
                 if (!engine_started_) {
+                    if (tuning_pending_) {  // set before the first request: the wavefront starts with it
+                        engine_->set_tuning(pending_tuning_);
+                        tuning_pending_ = false;
+                    }
                     engine_->begin(d_scenes_.ptr, d_views_.ptr, int(views_.size()));
                     engine_started_ = true;
                 }

@@ -238,29 +238,33 @@ __device__ __forceinline__ void walk_queue(uint32_t n, uint32_t* claim, uint32_t
 }
 
 // ---- the pair walk -----------------------------------------------------------------------------------
-// A warp's shared memory in the pair walk (512 bytes after the block's stacks): the owners' result
-// slots. (The owners' rays reach the testing lanes by shuffles: shared memory taken here is L1 cache
-// lost to the node and triangle reads.)
+// A warp's shared memory in the pair walk (2,048 bytes after the block's stacks): each lane's PairLane
+// slots and the owners' result slots of a pair pass.
 struct PairSlots {
+    float4 ray[32];
+    int4 leaves[32];
+    float4 hit[32];
     unsigned long long best[32];  // nearest accepted pair: distance bits << 32 | pair (any-hit: pair); ~0 none
     float2 uv[32];                // barycentrics of the pair a lane accepted
+    __device__ __forceinline__ PairLane lane(uint32_t l) { return PairLane{ray[l], leaves[l], hit[l]}; }
 };
-static_assert(sizeof(PairSlots) == 512, "PairSlots layout");
+static_assert(sizeof(PairSlots) == 2048, "PairSlots layout");
 
 // Tests the leaf pairs of a warp's lanes. Lane k, whose last node visit found m_k leaf triangles, owns
 // pairs [first_k, first_k + m_k) of the warp's list (an exclusive scan of m). The lanes take the list
 // 32 pairs at a time: lane j finds the owner of pair base + j by a binary search of the inclusive scan,
-// takes its ray and leaf ranges by shuffles (`scene`: the lane's own scene, in multi-scene launches),
-// tests that triangle against the owner's tmax, and an accepted pair enters the owner's slot by a
+// takes its origin by shuffles and its direction, tmax and leaf ranges from its slots (`scene`: the
+// lane's own scene, in multi-scene launches), tests that triangle against the owner's tmax, and an
+// accepted pair enters the owner's slot by a
 // 64-bit atomicMin of (distance bits << 32 | pair index): positive distances order as their bits, so
 // the owner gets its least distance, on a tie its earliest pair. A sequential leaf walk (traverse.h
 // :93-104) accepts a triangle only when it lowers tmax, so it ends on the first pair of least distance
 // below the entering tmax: the same triangle, distance and barycentrics. Any-hit keys are the pair
 // index alone (the first accepted pair, where the sequential walk stops). An owner whose pairs span two
 // rounds enters the second with its lowered tmax (an answered any-hit ray with 0, which accepts
-// nothing).
+// nothing). Returns whether the lane's own ray got a hit (any-hit: its answer).
 template <bool AnyHit, bool Count, bool Single, typename W>
-__device__ __forceinline__ void pair_pass(W& w, uint32_t m, PairSlots& ps, const WalkScene& uniform, const DevScene* scene,
+__device__ __forceinline__ bool pair_pass(W& w, uint32_t m, PairSlots& ps, const WalkScene& uniform, const DevScene* scene,
                                           TraversalCounters& tc) {
     const uint32_t lane = lane_id();
     uint32_t incl = m;
@@ -270,8 +274,13 @@ __device__ __forceinline__ void pair_pass(W& w, uint32_t m, PairSlots& ps, const
         if (lane >= s) incl += x;
     }
     const uint32_t total = __shfl_sync(kFull, incl, 31), first = incl - m;
+    if (m) {
+        ps.ray[lane].w = w.tmax;
+        ps.leaves[lane].w = int(first);
+    }
+    __syncwarp();
     const V3 o = w.origin();
-    float tmax = w.tmax;
+    bool answered = false;
     for (uint32_t base = 0; base < total; base += 32) {
         const uint32_t p = base + lane;
         uint32_t k = 0;
@@ -280,20 +289,18 @@ __device__ __forceinline__ void pair_pass(W& w, uint32_t m, PairSlots& ps, const
             if (__shfl_sync(kFull, incl, k + s - 1) <= p) k += s;
         }
         const V3 ko{__shfl_sync(kFull, o.x, k), __shfl_sync(kFull, o.y, k), __shfl_sync(kFull, o.z, k)};
-        const V3 kd{__shfl_sync(kFull, w.d.x, k), __shfl_sync(kFull, w.d.y, k), __shfl_sync(kFull, w.d.z, k)};
-        const float kt = __shfl_sync(kFull, tmax, k);
-        const int j = int(p - __shfl_sync(kFull, first, k));
-        const int kn0 = __shfl_sync(kFull, w.n0, k), kl0 = __shfl_sync(kFull, w.l0, k), kl1 = __shfl_sync(kFull, w.l1, k);
         const DevScene* sc = Single ? uniform.scene : reinterpret_cast<const DevScene*>(__shfl_sync(kFull, reinterpret_cast<unsigned long long>(scene), k));
         if (p < total) {
-            const int i = j < kn0 ? kl0 + j : kl1 + (j - kn0);
+            const float4 kr = ps.ray[k];
+            const int4 lv = ps.leaves[k];
+            const int i = pair_triangle(lv, int(p) - lv.w);
             const float4* g = (Single ? uniform.tris : sc->tris) + kTriStride * i;
             float4 g0, g1;
             ldg_pair(g, g0, g1);
             const float4 g2 = __ldg(g + 2);  // the record's fourth float4 is padding
             float t, tu, tv;
             if (Count) tc.tris++;
-            if (tri_intersect(g0, g1, g2, ko, kd, kt, t, tu, tv) &&
+            if (tri_intersect(g0, g1, g2, ko, xyz(kr), kr.w, t, tu, tv) &&
                 !((__float_as_int(g1.w) & 1) && alpha_passes(*sc, i, __float_as_int(g0.w), tu, tv))) {
                 const unsigned long long key = AnyHit ? (unsigned long long)p : ((unsigned long long)__float_as_uint(t) << 32 | p);
                 atomicMin(&ps.best[k], key);
@@ -306,18 +313,17 @@ __device__ __forceinline__ void pair_pass(W& w, uint32_t m, PairSlots& ps, const
             if (key != ~0ull) {
                 ps.best[lane] = ~0ull;
                 const uint32_t pw = uint32_t(key);
-                w.tri = w.pair_triangle(pw - first);
-                if (!AnyHit) {
-                    w.tmax = __uint_as_float(uint32_t(key >> 32));
-                    const float2 uv = ps.uv[pw - base];
-                    w.u = uv.x;
-                    w.v = uv.y;
-                }
-                tmax = AnyHit ? 0.0f : w.tmax;
+                const int tri = pair_triangle(ps.leaves[lane], int(pw - first));
+                const float2 uv = AnyHit ? make_float2(0.0f, 0.0f) : ps.uv[pw - base];
+                ps.hit[lane] = make_float4(__int_as_float(tri), uv.x, uv.y, 0.0f);
+                if (!AnyHit) w.tmax = __uint_as_float(uint32_t(key >> 32));
+                ps.ray[lane].w = AnyHit ? 0.0f : w.tmax;
+                answered = true;
             }
         }
         __syncwarp();
     }
+    return answered;
 }
 
 // Persistent walk over a ray queue in warp steps of the pair walk: in each of `visits` rounds, every
@@ -327,7 +333,8 @@ __device__ __forceinline__ void pair_pass(W& w, uint32_t m, PairSlots& ps, const
 // lanes as it has triangles, instead of the triangle tests of a few lanes running beside the node
 // visits of the others. (A warp-wide vote in the rounds, to end them once enough lanes wait, measured
 // slower: the rounds then reconverge the warp after every visit.) Refill, begin and end as in
-// walk_queue, checked once per step. Count: tc.steps counts node visits and warp_steps the rounds.
+// walk_queue, checked once per step; begin(i, w, ws, lane slots) and end(record, w, hit slot).
+// Count: tc.steps counts node visits and warp_steps the rounds.
 template <typename W, int Overflow, bool AnyHit, bool Count, bool Single, typename Begin, typename End>
 __device__ __forceinline__ void walk_queue_pairs(uint32_t n, uint32_t* claim, uint32_t refill, uint32_t visits, int* stack, int stride,
                                                  PairSlots& ps, const WalkScene& uniform, TraversalCounters& tc, uint32_t& warp_steps,
@@ -338,6 +345,7 @@ __device__ __forceinline__ void walk_queue_pairs(uint32_t n, uint32_t* claim, ui
     uint32_t idx = 0;
     bool live = false, drained = false;
     const uint32_t lane = lane_id(), below = (1u << lane) - 1u;
+    const PairLane sl = ps.lane(lane);
     ps.best[lane] = ~0ull;
     for (;;) {
         uint32_t act = __ballot_sync(kFull, live);
@@ -350,7 +358,7 @@ __device__ __forceinline__ void walk_queue_pairs(uint32_t n, uint32_t* claim, ui
             if (!live) {
                 const uint32_t r = base + uint32_t(__popc(idle & below));
                 if (r < n) {
-                    idx = begin(r, w, ws);
+                    idx = begin(r, w, ws, sl);
                     live = true;
                 }
             }
@@ -358,21 +366,22 @@ __device__ __forceinline__ void walk_queue_pairs(uint32_t n, uint32_t* claim, ui
         }
         if (act == 0) break;
         uint32_t m = 0;
+        NodeChoice ch;  // of a visit that waits for its leaf tests
         for (uint32_t it = 0; it < visits; it++) {
             if (live && m == 0) {
-                m = w.visit(Single ? uniform.nodes : ws.nodes, &tc);
+                m = w.visit(Single ? uniform.nodes : ws.nodes, sl, ch, &tc);
                 if (Count) tc.steps++;
-                if (m == 0 && !w.decide(stack, stride, overflow)) {
-                    end(idx, w);
+                if (m == 0 && !w.decide(ch, stack, stride, overflow)) {
+                    end(idx, w, sl.hit);
                     live = false;
                 }
             }
             if (Count) warp_steps++;
         }
         if (__any_sync(kFull, m != 0)) {
-            pair_pass<AnyHit, Count, Single>(w, m, ps, uniform, ws.scene, tc);
-            if (m && ((AnyHit && w.tri >= 0) || !w.decide(stack, stride, overflow))) {
-                end(idx, w);
+            const bool answered = pair_pass<AnyHit, Count, Single>(w, m, ps, uniform, ws.scene, tc);
+            if (m && ((AnyHit && answered) || !w.decide(ch, stack, stride, overflow))) {
+                end(idx, w, sl.hit);
                 live = false;
             }
         }
@@ -383,8 +392,7 @@ __device__ __forceinline__ void walk_queue_pairs(uint32_t n, uint32_t* claim, ui
 // server: each ray's scene comes from its view).
 __device__ __forceinline__ WalkScene single_walk_scene(const WfParams& P, bool wide) {
     if (P.single_scene < 0) return WalkScene{nullptr, nullptr, nullptr};
-    const DevScene& s = P.scenes[P.single_scene];
-    return WalkScene{wide ? s.nodes4 : s.nodes, s.tris, &s};
+    return WalkScene{wide ? P.single_nodes4 : P.single_nodes, P.single_tris, P.scenes + P.single_scene};
 }
 
 // ---- trace: closest hit (traverse.h:140-142) -------------------------------------------------------
@@ -432,7 +440,9 @@ __global__ void __maxnreg__(56) k_trace(const __grid_constant__ WfParams P) {
 }
 
 // The closest-hit walk as a pair walk (walk_queue_pairs): the same hits as k_trace. Dynamic shared
-// memory: the stacks, then one PairSlots per warp.
+// memory: the stacks, then one PairSlots per warp. Capped at 72 registers, where it needs no spills
+// (at 56, nine blocks of 128 threads per SM instead of seven, its spill traffic through L1 evicted node
+// lines: 24 MB of local stores per 960x540 bounce; 1080p frame 24.8 -> 24.4 ms with the higher cap).
 template <bool Count, bool Single>
 __global__ void __maxnreg__(56) k_trace_pairs(const __grid_constant__ WfParams P) {
     extern __shared__ int smem_stack[];
@@ -444,18 +454,18 @@ __global__ void __maxnreg__(56) k_trace_pairs(const __grid_constant__ WfParams P
     TraversalCounters tc{0, 0, 0};
     uint32_t warp_steps = 0;
     using W = PairWalker<false, Count>;
-    auto end = [&](uint32_t i, const W& w) {
-        P.pb.hit[i] = w.tri >= 0 ? make_float4(w.tmax, __int_as_float(w.tri), w.u, w.v) : make_float4(kInf, __int_as_float(-1), 0.0f, 0.0f);
+    auto end = [&](uint32_t i, const W& w, const float4& h) {
+        P.pb.hit[i] = __float_as_int(h.x) >= 0 ? make_float4(w.tmax, h.x, h.y, h.z) : make_float4(kInf, __int_as_float(-1), 0.0f, 0.0f);
     };
     const WalkScene uni = single_walk_scene(P, false);
     walk_queue_pairs<W, kStackSize - kSmemStack, false, Count, Single>(
         n, &c->fetch[1], P.trace_refill, P.pair_visits, stack, blockDim.x, ps, uni, tc, warp_steps,
-        [&](uint32_t i, W& w, WalkScene& ws) {
+        [&](uint32_t i, W& w, WalkScene& ws, const PairLane& sl) {
             if (!Single) {
                 const DevScene& s = P.scenes[P.views[P.pb.id[p][i].x].scene];
                 ws = WalkScene{s.nodes, s.tris, &s};
             }
-            w.init(xyz(P.pb.o[p][i]), xyz(P.pb.d[p][i]), kInf);
+            w.init(xyz(P.pb.o[p][i]), xyz(P.pb.d[p][i]), kInf, sl);
             return i;
         },
         end);
@@ -886,7 +896,7 @@ __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfPar
     const ShadowQueue sq{P, c->parity ^ 1u, c->shadow_sorting != 0};
     auto deliver = [&](uint32_t i) { sq.deliver(i); };
     auto init = [&](uint32_t i, auto& w) { return sq.init(i, w); };
-    if (Wide && Single && P.scenes[P.single_scene].nodes4) {
+    if (Wide && Single && P.single_nodes4) {
         using W4 = AnyWalker4<Count, Packed>;
         walk_queue<W4, kBvh4Stack - kSmemStack, Count, true>(
             n, &c->fetch[3], P.shadow_refill, P.walk_burst, stack, blockDim.x, single_walk_scene(P, true), tc, warp_steps,
@@ -923,6 +933,7 @@ __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfPar
 }
 
 // The any-hit walk as a pair walk (walk_queue_pairs) over the BVH2: the same answers as k_shadow.
+// Capped at 72 registers as k_trace_pairs (11.7 -> 11.5 ms per 1080p frame against 56).
 template <bool Count, bool Single>
 __global__ void __maxnreg__(56) k_shadow_pairs(const __grid_constant__ WfParams P) {
     extern __shared__ int smem_stack[];
@@ -937,16 +948,18 @@ __global__ void __maxnreg__(56) k_shadow_pairs(const __grid_constant__ WfParams 
     using W = PairWalker<true, Count>;
     walk_queue_pairs<W, kStackSize - kSmemStack, true, Count, Single>(
         n, &c->fetch[3], P.shadow_refill, P.pair_visits, stack, blockDim.x, ps, single_walk_scene(P, false), tc, warp_steps,
-        [&](uint32_t i, W& w, WalkScene& ws) {
-            const uint32_t j = sq.init(i, w);
+        [&](uint32_t i, W& w, WalkScene& ws, const PairLane& sl) {
+            const uint32_t j = sq.record(i);
+            const float4 a = P.pb.sh0[j];
+            w.init(xyz(a), xyz(P.pb.sh1[j]), a.w, sl);
             if (!Single) {
                 const DevScene& s = sq.scene(j);
                 ws = WalkScene{s.nodes, s.tris, &s};
             }
             return j;
         },
-        [&](uint32_t i, const W& w) {
-            if (w.tri < 0) sq.deliver(i);
+        [&](uint32_t i, const W&, const float4& h) {
+            if (__float_as_int(h.x) < 0) sq.deliver(i);
         });
     if (Count) {
         warp_add_u64(&c->shadow_node_visits, tc.nodes);

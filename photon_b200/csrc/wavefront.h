@@ -81,6 +81,9 @@ struct WfParams {
     const DevView* views;
     int num_views;
     int single_scene;          // >= 0: every view uses this scene slot
+    const float4* single_nodes;   // with single_scene >= 0: that scene's BVH2, 4-wide BVH (or null) and
+    const float4* single_nodes4;  // triangles, so that the walks take the array bases from the launch
+    const float4* single_tris;    // parameters instead of holding them in registers
     PathBuffers pb;
     Counters* ctr;
     int count_work;            // 1: count node visits / triangle tests (stats runs)

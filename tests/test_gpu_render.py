@@ -220,14 +220,20 @@ def test_gpu_matches_golden_fixtures(renderer, name):
     dict(tail_paths=0, trace_refill=32, shadow_refill=32),
     dict(tail_paths=0, trace_refill=5, shadow_refill=27, path_capacity=1 << 13),
     dict(tail_paths=0, wide_shadows=1, shadow_refill=32, trace_block=256),
+    dict(tail_paths=0, pair_walk=0),
+    dict(tail_paths=0, pair_walk=1),
+    dict(tail_paths=0, pair_walk=64, trace_refill=32, shadow_refill=1),
+    dict(tail_paths=0, pair_walk=3, trace_block=256, path_capacity=1 << 13),
+    dict(tail_paths=0, pair_walk=2, packed=0),
 ])
 def test_tuning_variants_are_bit_identical(tuning):
     """Every autotuner knob changes how the work is scheduled, never a path's arithmetic: scalar or
     packed slab tests, material-sorted shading, ray sorting, block shapes, the path pool size, the
     graph cadence, the one-thread-per-path tail (never, always, small), the shadow rays' BVH (4-wide
-    or Photon's BVH2) and when a walk's warp refills its idle lanes (only once all have finished,
-    whenever one has, in between) all give the same image bit for bit (accumulation is in sample
-    order). The variants that switch the tail off make the queued kernels walk every ray."""
+    or Photon's BVH2), when a walk's warp refills its idle lanes (only once all have finished,
+    whenever one has, in between) and whether leaf triangles are tested by their own lane or by the
+    warp's pair pass (after 1 to 64 node visits) all give the same image bit for bit (accumulation is
+    in sample order). The variants that switch the tail off make the queued kernels walk every ray."""
     desc, camf, keep = scenes.scene("terrain")
     w, h, spp = 160, 90, 4
     cam = camf(w / h)

@@ -59,6 +59,30 @@ def test_batched_views_with_split_passes_are_unchanged():
     r.close()
 
 
+@pytest.mark.parametrize("pair_walk", [0, 5])
+def test_server_walks_equal_the_renderer(pair_walk):
+    """The server's multi-scene walk kernels (each ray's scene from its view), as pair walks or per-lane
+    walks, give the image of the renderer's single-scene per-lane walk bit for bit. 320x180x4 paths
+    exceed the server's tail threshold, so the queued walks run."""
+    desc, camf, keep = scenes.scene("terrain")
+    cam, path = camf(16 / 9), abi.path_options(max_depth=12)
+    rr = native.Renderer()
+    rr.upload(desc)
+    rr.resize(320, 180)
+    rr.set_tuning(pair_walk=0, tail_paths=0)
+    rr.render(cam, abi.RenderSettings(320, 180, path, 1.0, abi.PT_TONEMAP_ACES, 4), 4)
+    want = rr.download_image()
+    rr.close()
+    s = native.Server(budget_bytes=8 << 30, path_capacity=1 << 18)
+    s.set_tuning(pair_walk=pair_walk)
+    sid = s.add_scene(desc)
+    rid = s.submit(sid, cam, 320, 180, 4, 4, path)
+    s.wait(rid, 60)
+    img, _ = s.fetch(rid, 320, 180)
+    s.close()
+    assert np.array_equal(img.view(np.uint32), want.view(np.uint32))
+
+
 @pytest.fixture(scope="module")
 def server_scenes():
     box = scenes.scene("box")
@@ -319,7 +343,7 @@ def test_autotuner_record_is_used_by_batches_and_the_server():
                             probe_samples=1 << 16)
     assert t1 >= d1 > 0
     r.close()
-    knobs = ("sort_by_material", "sort_rays", "packed", "wide_shadows", "trace_refill", "shadow_refill", "walk_burst")
+    knobs = ("sort_by_material", "sort_rays", "packed", "wide_shadows", "trace_refill", "shadow_refill", "walk_burst", "pair_walk")
     images = []
     for record in (None, {k: chosen[k] for k in knobs}):
         s = native.Server(budget_bytes=8 << 30, path_capacity=1 << 18)
