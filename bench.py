@@ -39,11 +39,17 @@ WORKLOAD = "262,144-triangle terrain scene (value-noise height field + 200 insta
            "64 emitters, 4 punctual lights, 1024x512 HDR sky), 1920x1080, 16 spp, max depth 12, seed 1"
 # Algorithmic bytes of the traversal kernels: one 64-byte node per visit, one 48-byte triangle per test.
 NODE_BYTES, TRI_BYTES = 64, 48
-# DRAM bytes (read + write) per traced ray of k_trace: the first k_trace launch of the 960x540x4 profile
-# case of the same scene (photon_b200/profile_case.py; 2,073,600 camera rays, 74.59 MB read + 11.79 MB
-# written in one ncu capture), scaled by the rays of a launch here: mostly the path state streaming in
-# and the hits out; the nodes and triangles stay in L2.
-TRACE_DRAM_BYTES_PER_RAY = (74.59e6 + 11.79e6) / 2073600
+# DRAM bytes (read + write) per traced ray of the closest-hit walk: its first launch in the 960x540x4
+# profile case of the same scene (photon_b200/profile_case.py; 2,073,600 camera rays, 75.60 MB read +
+# 11.98 MB written in one ncu capture), scaled by the rays of a launch here: mostly the path state
+# streaming in and the hits out; the nodes and triangles stay in L2.
+TRACE_DRAM_BYTES_PER_RAY = (75.60e6 + 11.98e6) / 2073600
+# Active threads per warp instruction (smsp__thread_inst_executed_per_inst_executed) of the pair walks
+# in the same capture (ncu --set full on python -m photon_b200.profile_case): the camera rays' launch,
+# then the first two bounces. The per-lane walks it replaced ran at 11.9 / 8.1 / 7.0 (closest hit) and
+# 7.7 / 6.1 / 5.8 (any hit) on the same case.
+NCU_THREADS_PER_INSTRUCTION = {"trace": [17.9, 15.1, 13.7], "shadow": [14.7, 12.6, 12.1], "of": 32,
+                               "per_lane_walks": {"trace": [11.9, 8.1, 7.0], "shadow": [7.7, 6.1, 5.8]}}
 # Workload description shared by both arms (the reference arm renders a bounded sample of it).
 CONFIG = {"workload": WORKLOAD, "scene_triangles": TRIS, "width": WIDTH, "height": HEIGHT, "spp": SPP, "max_depth": DEPTH,
           "samples_per_step": WIDTH * HEIGHT * SPP,
@@ -449,8 +455,9 @@ def main():
     # is kept beside it because the copy bandwidth is the measured peak of the schema.
     l2_peak = native.l2_read_bandwidth(local)
     closest_rays_frame = counts.closest_rays  # the counted render is one frame
+    pairs = r.tuning()["pair_walk"] > 0
     roofline = {"bound": "hbm", "limiter": "L2/L1 latency and issue: the scene is L2-resident (see l2, simt)",
-                "kernel": "k_trace (closest-hit BVH traversal)",
+                "kernel": "k_trace_pairs (closest-hit BVH traversal, pair walk)" if pairs else "k_trace (closest-hit BVH traversal)",
                 "l2": {"achieved": achieved, "peak": l2_peak, "unit": "GB/s", "frac": achieved / l2_peak if l2_peak > 0 else None,
                        "peak_source": "live pt_measure_l2_bandwidth: 32 MiB L2-resident buffer read 64 times per launch "
                                       "(ld.global.cg), best of 5"},
@@ -464,11 +471,14 @@ def main():
                 "model": "64 B per node visit + 48 B per triangle test (closest-hit rays)",
                 "node_visits_per_ray": counts.closest_node_visits / max(1, counts.closest_rays),
                 "tri_tests_per_ray": counts.closest_tri_tests / max(1, counts.closest_rays),
-                # Live SIMT use of the two walks from the counted render: live lanes per walk step, of 32.
-                "simt": {"trace_lanes_per_step": counts.closest_lane_steps / max(1, counts.closest_warp_steps),
-                         "shadow_lanes_per_step": counts.shadow_lane_steps / max(1, counts.shadow_warp_steps),
-                         "of": 32},
-                "shadow": {"kernel": "k_shadow (any-hit BVH traversal)", "bytes_per_frame": shadow_bytes_per_frame,
+                # SIMT use of the two walks: from the counted render, the lanes that visit a node per
+                # node-visit round of a pair walk (per walk step of a per-lane walk), of 32; from the
+                # profile capture, the active threads per warp instruction.
+                "simt": {"trace_lanes_per_round" if pairs else "trace_lanes_per_step": counts.closest_lane_steps / max(1, counts.closest_warp_steps),
+                         "shadow_lanes_per_round" if pairs else "shadow_lanes_per_step": counts.shadow_lane_steps / max(1, counts.shadow_warp_steps),
+                         "of": 32, "ncu_threads_per_instruction": NCU_THREADS_PER_INSTRUCTION},
+                "shadow": {"kernel": "k_shadow_pairs (any-hit BVH traversal, pair walk)" if pairs else "k_shadow (any-hit BVH traversal)",
+                           "bytes_per_frame": shadow_bytes_per_frame,
                            "ms_per_frame": prof.shadow.ms / args.steps, "achieved": shadow_achieved,
                            "l2_frac": shadow_achieved / l2_peak if l2_peak > 0 else None, "hbm_frac": shadow_achieved / peak}}
     rays_per_sample = (counts.closest_rays + counts.shadow_rays) / samples_per_step
