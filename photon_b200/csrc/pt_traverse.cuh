@@ -363,6 +363,82 @@ struct PairWalker {
 // The triangle of pair j of a visit whose leaf ranges are lv (PairLane::leaves).
 PT_HD int pair_triangle(const int4& lv, int j) { return j < lv.y ? lv.x + j : lv.z + (j - lv.y); }
 
+// The any-hit pair walk over the 4-wide BVH (wide_bvh.h): whether some triangle accepts the ray is
+// order-free, and the 4-wide tree reaches the BVH2's leaves (see AnyWalker4), so the answer is the
+// BVH2 walk's. A visit tests the four children of the current node, pushes the inner ones it enters and
+// then its leaf children (so leaves come off the stack first), and pops the next entry; an entry that
+// is a leaf is handed to the warp's pair pass as the lane's one leaf range. Half as many dependent node
+// reads as the BVH2 walk, at four slab tests per read.
+template <bool Count>
+struct PairWalker4 {
+    RaySlab rs;
+    float tmax;
+    int cur;   // the current entry: a node index, or a leaf as 0x80000000 | count << 24 | first triangle
+    int sp;    // -1 once the stack ran out (the ray is finished)
+
+    PT_HD void init(V3 o_, V3 d_, float tmax_, const PairLane& sl) {
+        rs = ray_slab(o_, V3{safe_inv(d_.x), safe_inv(d_.y), safe_inv(d_.z)});
+        tmax = tmax_;
+        cur = 0;
+        sp = 0;
+        sl.ray = make_float4(d_.x, d_.y, d_.z, tmax_);
+        sl.hit = make_float4(__int_as_float(-1), 0.0f, 0.0f, 0.0f);
+    }
+    PT_HD V3 origin() const {
+        float x, y;
+        unpack2(rs.oxy, x, y);
+        return V3{x, y, rs.oz};
+    }
+    PT_HD void push(int e, int* stack, int stride, int* overflow) {
+        if (sp < kSmemStack) stack[sp * stride] = e;
+        else overflow[sp - kSmemStack] = e;
+        sp++;
+    }
+    // Pops the next entry into cur; false once the stack is empty.
+    PT_HD bool pop(int* stack, int stride, int* overflow) {
+        if (sp == 0) {
+            sp = -1;
+            return false;
+        }
+        --sp;
+        cur = sp < kSmemStack ? stack[sp * stride] : overflow[sp - kSmemStack];
+        return true;
+    }
+    // The current entry's triangles if it is a leaf (its range into the lane's slot), else 0.
+    PT_HD uint32_t leaf_pairs(const PairLane& sl) const {
+        if (cur >= 0) return 0;
+        const int n = (cur >> 24) & 0x7f;
+        sl.leaves = make_int4(cur & 0xffffff, n, 0, 0);
+        return uint32_t(n);
+    }
+    // Visits the current node (cur >= 0) and pops the next entry; false once the ray is finished.
+    PT_HD bool visit(const float4* nodes4, int* stack, int stride, int* overflow, TraversalCounters* cnt) {
+        const float4* n = nodes4 + 8 * cur;  // 128-byte nodes: four 256-bit loads
+        float4 lx, ly, lz, hx, hy, hz, id4, ct4;
+        ldg_pair(n, lx, ly);
+        ldg_pair(n + 2, lz, hx);
+        ldg_pair(n + 4, hy, hz);
+        ldg_pair(n + 6, id4, ct4);
+        if (Count) cnt->nodes++;
+        const float lxs[4] = {lx.x, lx.y, lx.z, lx.w}, lys[4] = {ly.x, ly.y, ly.z, ly.w}, lzs[4] = {lz.x, lz.y, lz.z, lz.w};
+        const float hxs[4] = {hx.x, hx.y, hx.z, hx.w}, hys[4] = {hy.x, hy.y, hy.z, hy.w}, hzs[4] = {hz.x, hz.y, hz.z, hz.w};
+        const int ids[4] = {__float_as_int(id4.x), __float_as_int(id4.y), __float_as_int(id4.z), __float_as_int(id4.w)};
+        const int cts[4] = {__float_as_int(ct4.x), __float_as_int(ct4.y), __float_as_int(ct4.z), __float_as_int(ct4.w)};
+        int leaves[4];
+        int nl = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (ids[k] < 0) continue;
+            const float t = box_entry3(make_float4(lxs[k], lys[k], lzs[k], 0.0f), make_float4(hxs[k], hys[k], hzs[k], 0.0f), rs, tmax);
+            if (t == kInf) continue;
+            if (cts[k] > 0) leaves[nl++] = int(0x80000000u | (uint32_t(cts[k]) << 24) | uint32_t(ids[k]));
+            else if (t < tmax) push(ids[k], stack, stride, overflow);
+        }
+        for (int k = 0; k < nl; k++) push(leaves[k], stack, stride, overflow);
+        return pop(stack, stride, overflow);
+    }
+};
+
 // One ray's traversal: AnyHit stops at the first accepted triangle. `stack` is this thread's column of
 // the block's shared stack (entry k at stack[k * stride]).
 template <bool AnyHit, bool Count, bool Packed = true>

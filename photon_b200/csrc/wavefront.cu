@@ -388,6 +388,67 @@ __device__ __forceinline__ void walk_queue_pairs(uint32_t n, uint32_t* claim, ui
     }
 }
 
+// The any-hit pair walk over the 4-wide BVH (PairWalker4): each round, a live lane without a leaf
+// waiting visits its current node and pops the next entry; a leaf entry waits for the step's pair pass,
+// after which the lane pops on (or ends: answered, or the stack ran out). Refill, begin and end as in
+// walk_queue_pairs; `uniform` carries the single scene's triangles (the 4-wide BVH is built for the
+// renderer's single scene only). Count: tc.steps counts node visits and warp_steps the rounds.
+template <int Overflow, bool Count, typename Begin, typename End>
+__device__ __forceinline__ void walk_queue_pairs4(uint32_t n, uint32_t* claim, uint32_t refill, uint32_t visits, int* stack, int stride,
+                                                  PairSlots& ps, const float4* nodes4, const WalkScene& uniform, TraversalCounters& tc,
+                                                  uint32_t& warp_steps, Begin begin, End end) {
+    int overflow[Overflow];
+    PairWalker4<Count> w;
+    WalkScene ws = uniform;
+    uint32_t idx = 0;
+    bool live = false, drained = false;
+    const uint32_t lane = lane_id(), below = (1u << lane) - 1u;
+    const PairLane sl = ps.lane(lane);
+    ps.best[lane] = ~0ull;
+    for (;;) {
+        uint32_t act = __ballot_sync(kFull, live);
+        if (!drained && uint32_t(__popc(act)) < refill) {
+            const uint32_t idle = ~act, want = uint32_t(__popc(idle));
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(claim, want);
+            base = __shfl_sync(kFull, base, 0);
+            drained = base + want >= n;
+            if (!live) {
+                const uint32_t r = base + uint32_t(__popc(idle & below));
+                if (r < n) {
+                    idx = begin(r, w, ws, sl);
+                    live = true;
+                }
+            }
+            act = __ballot_sync(kFull, live);
+        }
+        if (act == 0) break;
+        uint32_t m = 0;
+        for (uint32_t it = 0; it < visits; it++) {
+            if (live && m == 0) {
+                m = w.leaf_pairs(sl);
+                if (m == 0) {
+                    if (Count) tc.steps++;
+                    if (w.visit(nodes4, stack, stride, overflow, &tc)) {
+                        m = w.leaf_pairs(sl);
+                    } else {
+                        end(idx, w, sl.hit);
+                        live = false;
+                    }
+                }
+            }
+            if (Count) warp_steps++;
+        }
+        if (__any_sync(kFull, m != 0)) {
+            const bool answered = pair_pass<true, Count, true>(w, m, ps, uniform, uniform.scene, tc);
+            if (m && (answered || !w.pop(stack, stride, overflow))) {
+                end(idx, w, sl.hit);
+                live = false;
+            }
+        }
+    }
+}
+
 // The scene arrays of a launch whose views all use one scene (the renderer), or null arrays (the
 // server: each ray's scene comes from its view).
 __device__ __forceinline__ WalkScene single_walk_scene(const WfParams& P, bool wide) {
@@ -440,9 +501,10 @@ __global__ void __maxnreg__(56) k_trace(const __grid_constant__ WfParams P) {
 }
 
 // The closest-hit walk as a pair walk (walk_queue_pairs): the same hits as k_trace. Dynamic shared
-// memory: the stacks, then one PairSlots per warp. Capped at 72 registers, where it needs no spills
-// (at 56, nine blocks of 128 threads per SM instead of seven, its spill traffic through L1 evicted node
-// lines: 24 MB of local stores per 960x540 bounce; 1080p frame 24.8 -> 24.4 ms with the higher cap).
+// memory: the stacks, then one PairSlots per warp. 56 registers (nine blocks of 128 threads per SM),
+// where the single-scene kernels need no spills: spill traffic through L1 evicts node lines (24 MB of
+// local stores per 960x540 bounce when the walk kept more state in registers), and 64 or 72 registers
+// (eight or seven blocks) measured slower than 56 without spills.
 template <bool Count, bool Single>
 __global__ void __maxnreg__(56) k_trace_pairs(const __grid_constant__ WfParams P) {
     extern __shared__ int smem_stack[];
@@ -932,9 +994,9 @@ __global__ void __launch_bounds__(256, 5) k_shadow(const __grid_constant__ WfPar
     }
 }
 
-// The any-hit walk as a pair walk (walk_queue_pairs) over the BVH2: the same answers as k_shadow.
-// Capped at 72 registers as k_trace_pairs (11.7 -> 11.5 ms per 1080p frame against 56).
-template <bool Count, bool Single>
+// The any-hit walk as a pair walk (walk_queue_pairs) over the BVH2, or (Wide, where the single scene
+// carries one) over the 4-wide BVH (walk_queue_pairs4): the same answers as k_shadow.
+template <bool Count, bool Single, bool Wide>
 __global__ void __maxnreg__(56) k_shadow_pairs(const __grid_constant__ WfParams P) {
     extern __shared__ int smem_stack[];
     int* stack = smem_stack + threadIdx.x;
@@ -945,22 +1007,36 @@ __global__ void __maxnreg__(56) k_shadow_pairs(const __grid_constant__ WfParams 
     TraversalCounters tc{0, 0, 0};
     uint32_t warp_steps = 0;
     const ShadowQueue sq{P, c->parity ^ 1u, c->shadow_sorting != 0};
-    using W = PairWalker<true, Count>;
-    walk_queue_pairs<W, kStackSize - kSmemStack, true, Count, Single>(
-        n, &c->fetch[3], P.shadow_refill, P.pair_visits, stack, blockDim.x, ps, single_walk_scene(P, false), tc, warp_steps,
-        [&](uint32_t i, W& w, WalkScene& ws, const PairLane& sl) {
-            const uint32_t j = sq.record(i);
-            const float4 a = P.pb.sh0[j];
-            w.init(xyz(a), xyz(P.pb.sh1[j]), a.w, sl);
-            if (!Single) {
-                const DevScene& s = sq.scene(j);
-                ws = WalkScene{s.nodes, s.tris, &s};
-            }
-            return j;
-        },
-        [&](uint32_t i, const W&, const float4& h) {
-            if (__float_as_int(h.x) < 0) sq.deliver(i);
-        });
+    auto end = [&](uint32_t i, const auto&, const float4& h) {
+        if (__float_as_int(h.x) < 0) sq.deliver(i);
+    };
+    if (Wide && Single && P.single_nodes4) {
+        walk_queue_pairs4<kBvh4Stack - kSmemStack, Count>(
+            n, &c->fetch[3], P.shadow_refill, P.pair_visits, stack, blockDim.x, ps, P.single_nodes4, single_walk_scene(P, false), tc,
+            warp_steps,
+            [&](uint32_t i, PairWalker4<Count>& w, WalkScene&, const PairLane& sl) {
+                const uint32_t j = sq.record(i);
+                const float4 a = P.pb.sh0[j];
+                w.init(xyz(a), xyz(P.pb.sh1[j]), a.w, sl);
+                return j;
+            },
+            end);
+    } else {
+        using W = PairWalker<true, Count>;
+        walk_queue_pairs<W, kStackSize - kSmemStack, true, Count, Single>(
+            n, &c->fetch[3], P.shadow_refill, P.pair_visits, stack, blockDim.x, ps, single_walk_scene(P, false), tc, warp_steps,
+            [&](uint32_t i, W& w, WalkScene& ws, const PairLane& sl) {
+                const uint32_t j = sq.record(i);
+                const float4 a = P.pb.sh0[j];
+                w.init(xyz(a), xyz(P.pb.sh1[j]), a.w, sl);
+                if (!Single) {
+                    const DevScene& s = sq.scene(j);
+                    ws = WalkScene{s.nodes, s.tris, &s};
+                }
+                return j;
+            },
+            end);
+    }
     if (Count) {
         warp_add_u64(&c->shadow_node_visits, tc.nodes);
         warp_add_u64(&c->shadow_tri_tests, tc.tris);
@@ -1293,10 +1369,11 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
         if (e != cudaSuccess) return e;
     }
     const size_t pair_smem = smem + size_t(trace_block / 32) * sizeof(PairSlots);
-    const void* pair_kernels[] = {(const void*)k_trace_pairs<false, false>, (const void*)k_trace_pairs<false, true>,
-                                  (const void*)k_trace_pairs<true, false>,  (const void*)k_trace_pairs<true, true>,
-                                  (const void*)k_shadow_pairs<false, false>, (const void*)k_shadow_pairs<false, true>,
-                                  (const void*)k_shadow_pairs<true, false>,  (const void*)k_shadow_pairs<true, true>};
+    const void* pair_kernels[] = {(const void*)k_trace_pairs<false, false>,         (const void*)k_trace_pairs<false, true>,
+                                  (const void*)k_trace_pairs<true, false>,          (const void*)k_trace_pairs<true, true>,
+                                  (const void*)k_shadow_pairs<false, false, false>, (const void*)k_shadow_pairs<false, true, false>,
+                                  (const void*)k_shadow_pairs<true, false, false>,  (const void*)k_shadow_pairs<true, true, false>,
+                                  (const void*)k_shadow_pairs<false, true, true>,   (const void*)k_shadow_pairs<true, true, true>};
     for (const void* k : pair_kernels) {
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pair_smem));
         if (e != cudaSuccess) return e;
@@ -1304,7 +1381,7 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trace_pairs<false, false>, trace_block, pair_smem);
     if (e != cudaSuccess) return e;
     out->pair_trace_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shadow_pairs<false, false>, trace_block, pair_smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shadow_pairs<false, false, false>, trace_block, pair_smem);
     if (e != cudaSuccess) return e;
     out->pair_shadow_grid = prop.multiProcessorCount * (nb > 0 ? nb : 1);
     // Grids are sized for the heavier (multi-scene) variants, so that every variant's grid fits.
@@ -1324,9 +1401,10 @@ cudaError_t wf_launch_shape(int device, int trace_block, int shade_block, Launch
 
 template <bool Count, bool Packed, bool Single>
 static void launch_traversals(const WfParams& p, const LaunchShape& ls, cudaStream_t stream, size_t smem, bool shadow) {
-    if (Packed && p.pair_visits > 0 && !(shadow && p.wide_shadows)) {
+    if (Packed && p.pair_visits > 0) {
         const size_t pair_smem = smem + size_t(ls.trace_block / 32) * sizeof(PairSlots);
-        if (shadow) k_shadow_pairs<Count, Single><<<ls.pair_shadow_grid, ls.shadow_block, pair_smem, stream>>>(p);
+        if (shadow && Single && p.wide_shadows) k_shadow_pairs<Count, true, true><<<ls.pair_shadow_grid, ls.shadow_block, pair_smem, stream>>>(p);
+        else if (shadow) k_shadow_pairs<Count, Single, false><<<ls.pair_shadow_grid, ls.shadow_block, pair_smem, stream>>>(p);
         else k_trace_pairs<Count, Single><<<ls.pair_trace_grid, ls.trace_block, pair_smem, stream>>>(p);
         return;
     }
