@@ -153,11 +153,15 @@ void DeviceScene::upload(const pt_scene_desc& d, cudaStream_t s, bool lights_onl
     // What update_lights re-uploads (gpu_renderer.cu:303-310): triangles, materials, light tables
     // and the environment.
     {
-        // Photon's 48-byte TriGeom records, each padded to 64 bytes (kTriStride float4).
+        // Photon's 48-byte TriGeom records, each padded to 64 bytes (kTriStride float4); the padding
+        // carries the vertex indices for the alpha test.
         std::vector<float4> padded(size_t(d.num_tris) * kTriStride, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
         const float4* src = reinterpret_cast<const float4*>(d.tris);
-        for (size_t t = 0; t < size_t(d.num_tris); t++)
+        for (size_t t = 0; t < size_t(d.num_tris); t++) {
             for (int k = 0; k < 3; k++) padded[t * kTriStride + size_t(k)] = src[t * 3 + size_t(k)];
+            int32_t vi[4] = {d.indices[3 * t], d.indices[3 * t + 1], d.indices[3 * t + 2], 0};
+            std::memcpy(&padded[t * kTriStride + 3], vi, sizeof(vi));
+        }
         tris_.upload(padded.data(), padded.size(), s);
         PTW_CUDA(cudaStreamSynchronize(s));
     }

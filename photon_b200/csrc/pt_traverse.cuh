@@ -210,7 +210,7 @@ struct Walker {
             float t, tu, tv;
             if (Count) cnt->tris++;
             if (tri_intersect(g0, g1, g2, o, d, tmax, t, tu, tv) &&
-                !((__float_as_int(g1.w) & 1) && alpha_passes(*ws.scene, i, __float_as_int(g0.w), tu, tv))) {
+                !((__float_as_int(g1.w) & 1) && alpha_passes(*ws.scene, g, __float_as_int(g0.w), tu, tv))) {
                 tmax = t;
                 tri = i;
                 u = tu;
@@ -551,7 +551,7 @@ struct AnyWalker4 {
             float t, tu, tv;
             if (Count) cnt->tris++;
             if (tri_intersect(g0, g1, g2, o, d, tmax, t, tu, tv) &&
-                !((__float_as_int(g1.w) & 1) && alpha_passes(*ws.scene, i, __float_as_int(g0.w), tu, tv))) {
+                !((__float_as_int(g1.w) & 1) && alpha_passes(*ws.scene, g, __float_as_int(g0.w), tu, tv))) {
                 hit = true;
                 done = true;
                 return false;

@@ -9,8 +9,9 @@ namespace ptw {
 
 // Scene arrays on the device. Layouts (all 16-byte aligned):
 //   nodes     4 x float4 per node: (lmin, left) (lmax, lcount) (rmin, right) (rmax, rcount)
-//   tris      kTriStride (4) x float4 per triangle: (v0, material) (e1, flags) (e2, pad) (unused)
-//             [BVH order]; 64 bytes each, so that a triangle is two aligned 256-bit loads
+//   tris      kTriStride (4) x float4 per triangle: (v0, material) (e1, flags) (e2, pad) (the vertex
+//             indices as int bits, 0) [BVH order]; 64 bytes each: the intersection test reads the
+//             first 48 with a 256-bit and a 128-bit load, the alpha test the indices from the same line
 //   tri_idx   int4 per triangle: (vertex 0, vertex 1, vertex 2, emissive entry or -1)
 //   normals   float4 per vertex (n, 0);  uvs float2 per vertex;  tangents float4 per vertex
 //   materials 5 x float4 per material: Photon's 80-byte Material read as five 16-byte words

@@ -301,7 +301,7 @@ __device__ __forceinline__ bool pair_pass(W& w, uint32_t m, PairSlots& ps, const
             float t, tu, tv;
             if (Count) tc.tris++;
             if (tri_intersect(g0, g1, g2, ko, xyz(kr), kr.w, t, tu, tv) &&
-                !((__float_as_int(g1.w) & 1) && alpha_passes(*sc, i, __float_as_int(g0.w), tu, tv))) {
+                !((__float_as_int(g1.w) & 1) && alpha_passes(*sc, g, __float_as_int(g0.w), tu, tv))) {
                 const unsigned long long key = AnyHit ? (unsigned long long)p : ((unsigned long long)__float_as_uint(t) << 32 | p);
                 atomicMin(&ps.best[k], key);
                 if (!AnyHit) ps.uv[lane] = make_float2(tu, tv);
