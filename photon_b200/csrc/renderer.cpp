@@ -648,6 +648,15 @@ void Renderer::resolve_and_copy_out(const float4* src, size_t npix, float scale,
     const size_t n = 3 * npix;
     rgb_dev_.reserve(n);
     PTW_CUDA(wf_resolve(src, uint32_t(npix), scale, apply_scale, rgb_dev_.ptr, stream_));
+    // A page-locked destination takes one direct copy at the link's rate; pageable memory goes
+    // through the pinned halves below.
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, rgb) == cudaSuccess && attr.type == cudaMemoryTypeHost) {
+        PTW_CUDA(cudaMemcpyAsync(rgb, rgb_dev_.ptr, n * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+        PTW_CUDA(cudaStreamSynchronize(stream_));
+        return;
+    }
+    cudaGetLastError();  // (an unknown pointer is not an error here)
     for (int k = 0; k < 2; k++) {
         if (!stage_[k]) PTW_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&stage_[k]), kChunk * sizeof(float), cudaHostAllocDefault));
         if (!stage_ev_[k]) PTW_CUDA(cudaEventCreateWithFlags(&stage_ev_[k], cudaEventDisableTiming));

@@ -345,3 +345,20 @@ def test_any_hit_walk_bit_exact(renderer, name):
     wide = renderer.occlusion_probe(rays, wide=True)
     assert np.array_equal(wide[:, 0], want[:, 0])
     assert 0.2 < got[:, 0].mean() < 0.95
+
+
+def test_download_into_page_locked_memory_equals_pageable():
+    """pt_download_image copies straight into a page-locked destination and through pinned staging
+    into pageable memory: the same bytes either way (an image larger than one staging half)."""
+    import torch
+    desc, camf, keep = scenes.scene("terrain")
+    w, h = 1280, 720
+    r = native.Renderer()
+    r.upload(desc)
+    r.resize(w, h)
+    r.render(camf(w / h), _settings("terrain", w, h, seed=2), 1)
+    pageable = r.download_image()
+    pinned = torch.empty((h, w, 3), dtype=torch.float32, pin_memory=True).numpy()
+    r.download_image(out=pinned)
+    r.close()
+    assert np.array_equal(pageable.view(np.uint32), pinned.view(np.uint32))
