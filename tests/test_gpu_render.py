@@ -362,3 +362,26 @@ def test_download_into_page_locked_memory_equals_pageable():
     r.download_image(out=pinned)
     r.close()
     assert np.array_equal(pageable.view(np.uint32), pinned.view(np.uint32))
+
+
+def test_pair_walk_visits_the_nodes_the_lane_walk_visits():
+    """The pair walks visit exactly the per-lane walks' nodes: the counted render's node visits of the
+    closest-hit and any-hit walks and the closest-hit triangle tests are equal (a pair walk tests a
+    node's leaf triangles together, where the per-lane any-hit walk stops at the first accepted one,
+    so only the any-hit triangle tests may differ), and so is the image."""
+    desc, camf, keep = scenes.scene("terrain")
+    w, h = 640, 360
+    counts, images = [], []
+    for pw in (0, 5):
+        r = native.Renderer()
+        r.upload(desc)
+        r.resize(w, h)
+        r.set_tuning(pair_walk=pw, tail_paths=0)
+        r.set_profiling(abi.PT_PROFILE_TRAVERSAL_COUNTS)
+        r.render(camf(w / h), _settings("terrain", w, h, seed=4), 2)
+        p = r.profile()
+        counts.append((p.closest_rays, p.closest_node_visits, p.closest_tri_tests, p.shadow_rays, p.shadow_node_visits))
+        images.append(r.download_image())
+        r.close()
+    assert counts[0] == counts[1] and counts[0][1] > 0 and counts[0][4] > 0
+    assert np.array_equal(images[0].view(np.uint32), images[1].view(np.uint32))
