@@ -40,15 +40,15 @@ WORKLOAD = "262,144-triangle terrain scene (value-noise height field + 200 insta
 # Algorithmic bytes of the traversal kernels: one 64-byte node per visit, one 48-byte triangle per test.
 NODE_BYTES, TRI_BYTES = 64, 48
 # DRAM bytes (read + write) per traced ray of the closest-hit walk: its first launch in the 960x540x4
-# profile case of the same scene (photon_b200/profile_case.py; 2,073,600 camera rays, 75.60 MB read +
-# 11.98 MB written in one ncu capture), scaled by the rays of a launch here: mostly the path state
+# profile case of the same scene (photon_b200/profile_case.py; 2,073,600 camera rays, 75.03 MB read +
+# 11.30 MB written in one ncu capture), scaled by the rays of a launch here: mostly the path state
 # streaming in and the hits out; the nodes and triangles stay in L2.
-TRACE_DRAM_BYTES_PER_RAY = (75.60e6 + 11.98e6) / 2073600
+TRACE_DRAM_BYTES_PER_RAY = (75.03e6 + 11.30e6) / 2073600
 # Active threads per warp instruction (smsp__thread_inst_executed_per_inst_executed) of the pair walks
 # in the same capture (ncu --set full on python -m photon_b200.profile_case): the camera rays' launch,
 # then the first two bounces. The per-lane walks it replaced ran at 11.9 / 8.1 / 7.0 (closest hit) and
 # 7.7 / 6.1 / 5.8 (any hit) on the same case.
-NCU_THREADS_PER_INSTRUCTION = {"trace": [17.9, 15.1, 13.7], "shadow": [14.7, 12.6, 12.1], "of": 32,
+NCU_THREADS_PER_INSTRUCTION = {"trace": [18.2, 15.4, 14.1], "shadow": [15.0, 13.0, 12.5], "of": 32,
                                "per_lane_walks": {"trace": [11.9, 8.1, 7.0], "shadow": [7.7, 6.1, 5.8]}}
 # Workload description shared by both arms (the reference arm renders a bounded sample of it).
 CONFIG = {"workload": WORKLOAD, "scene_triangles": TRIS, "width": WIDTH, "height": HEIGHT, "spp": SPP, "max_depth": DEPTH,
