@@ -311,7 +311,8 @@ int32_t pt_get_profile(const pt_renderer* r, pt_profile* out);
 
 /* Primary closest hits of pixel centres + the first random jitter of sample `frame`, exactly the
  * camera rays of render_sample (pixel.h:18-24): per pixel (t, tri, u, v) into hits4 (4 * w * h floats;
- * tri is stored as a float bit pattern of the int32, -1 on a miss). */
+ * tri is stored as a float bit pattern of the int32, -1 on a miss). Walked as the renderer's rendering
+ * walks them: the pair walk unless its tuning sets pair_walk = 0 (or packed = 0). */
 int32_t pt_trace_primary(pt_renderer* r, const pt_camera* camera, int32_t width, int32_t height, uint32_t frame,
                          uint32_t seed, float* hits4);
 /* The light pick of next event estimation at the first vertex of every pixel's sample `frame`
@@ -325,8 +326,10 @@ int32_t pt_light_picks_primary(pt_renderer* r, const pt_camera* camera, const pt
 int32_t pt_heatmap(pt_renderer* r, const pt_camera* camera, int32_t width, int32_t height, float* visits);
 /* Any-hit walks (traverse.h:144-147, occluded; the shadow rays' walk) of n caller rays, 8 floats each
  * (origin, tmax, direction, unused): out4 per ray = (occluded, first triangle accepted in the walk's
- * order or -1, node visits, triangle tests). wide = 1 walks the 4-wide BVH where the scene has one
- * (then only `occluded` is Photon's, the counts are of the 4-wide walk). */
+ * order or -1, node visits, triangle tests). Walked as the renderer's shadow rays are: the pair walk
+ * unless its tuning sets pair_walk = 0 (or packed = 0); a pair walk's triangle tests are made by other
+ * lanes and reported as -1. wide = 1 walks the 4-wide BVH where the scene has one (then only
+ * `occluded` is Photon's, the counts are of the 4-wide walk). */
 int32_t pt_occlusion_probe(pt_renderer* r, const float* rays8, int32_t n, int32_t wide, int32_t* out4);
 
 /* ---- batched views (one persistent launch over many views) --------------------------------- */

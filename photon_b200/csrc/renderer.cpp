@@ -916,7 +916,11 @@ void Renderer::trace_primary(const pt_camera& cam, int w, int h, uint32_t frame,
     PTW_CUDA(cudaSetDevice(device_));
     DeviceBuffer<float4> out;
     out.allocate(size_t(w) * size_t(h));
-    PTW_CUDA(wf_trace_primary(scene_.device_view(), reinterpret_cast<const float*>(&cam), w, h, frame, seed, out.ptr, stream_));
+    probe_claim_.reserve(1);
+    const Tuning& t = engine_->tuning();
+    const uint32_t pairs = t.packed ? uint32_t(std::clamp(t.pair_walk, 0, 64)) : 0u;  // the render's closest-hit walk
+    PTW_CUDA(wf_trace_primary(scene_.device_view(), reinterpret_cast<const float*>(&cam), w, h, frame, seed, out.ptr, probe_claim_.ptr, pairs,
+                              stream_));
     PTW_CUDA(cudaMemcpyAsync(hits4, out.ptr, out.bytes(), cudaMemcpyDeviceToHost, stream_));
     PTW_CUDA(cudaStreamSynchronize(stream_));
 }
@@ -955,7 +959,10 @@ void Renderer::occlusion_probe(const float* rays8, int n, int wide, int32_t* out
     rays.upload(reinterpret_cast<const float4*>(rays8), size_t(n) * 2, stream_);
     DeviceBuffer<int4> out;
     out.allocate(size_t(n));
-    PTW_CUDA(wf_occlusion_probe(scene_.device_view(), rays.ptr, n, wide, out.ptr, stream_));
+    probe_claim_.reserve(1);
+    const Tuning& t = engine_->tuning();
+    const uint32_t pairs = t.packed ? uint32_t(std::clamp(t.pair_walk, 0, 64)) : 0u;  // the render's any-hit walk
+    PTW_CUDA(wf_occlusion_probe(scene_.device_view(), rays.ptr, n, wide, out.ptr, probe_claim_.ptr, pairs, stream_));
     PTW_CUDA(cudaMemcpyAsync(out4, out.ptr, out.bytes(), cudaMemcpyDeviceToHost, stream_));
     PTW_CUDA(cudaStreamSynchronize(stream_));
 }

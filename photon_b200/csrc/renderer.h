@@ -202,6 +202,7 @@ private:
     DeviceBuffer<float4> accum_, acc_pass_, albedo_, normal_depth_, edge_, motion_, emission_, color_, denoised_buf_;
     DeviceBuffer<float> heat_;
     DeviceBuffer<uint32_t> display_;
+    DeviceBuffer<uint32_t> probe_claim_;  // the pair-walk probes' queue counter
     DeviceBuffer<float4> sample_out_;
     DeviceBuffer<DevView> d_views_;
     pt_camera last_camera_{};

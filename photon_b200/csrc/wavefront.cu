@@ -1242,6 +1242,59 @@ __global__ void __launch_bounds__(128) k_occlusion_probe(const DevScene* sp, con
     out[i] = make_int4(occ ? 1 : 0, occ ? h.tri : -1, int(tc.nodes), int(tc.tris));
 }
 
+// The probes above through the pair walks (walk_queue_pairs, PairWalker: the code of k_trace_pairs and
+// k_shadow_pairs) over a queue of the probe's rays, so that the default walks are pinned ray by ray:
+// the camera rays' hits, and per caller ray the occlusion, first accepted triangle and node visits (the
+// triangle tests of a pair walk are done by other lanes: reported as -1). `claim` is a zeroed counter.
+__global__ void __launch_bounds__(128) k_trace_primary_pairs(const DevScene* sp, CameraArg cam, int w, int h, uint32_t frame, uint32_t seed,
+                                                            float4* out, uint32_t* claim, uint32_t visits) {
+    extern __shared__ int smem_stack[];
+    PairSlots& ps = reinterpret_cast<PairSlots*>(smem_stack + kSmemStack * blockDim.x)[threadIdx.x >> 5];
+    const DevScene& s = *sp;
+    const WalkScene uni{s.nodes, s.tris, sp};
+    TraversalCounters tc{0, 0, 0};
+    uint32_t warp_steps = 0;
+    using W = PairWalker<false, false>;
+    walk_queue_pairs<W, kStackSize - kSmemStack, false, false, true>(
+        uint32_t(w) * uint32_t(h), claim, 24u, visits, smem_stack + threadIdx.x, blockDim.x, ps, uni, tc, warp_steps,
+        [&](uint32_t pixel, W& wk, WalkScene&, const PairLane& sl) {
+            const int x = int(pixel % uint32_t(w)), y = int(pixel / uint32_t(w));
+            Rng rng = pixel_rng(pixel, seed, frame);
+            V2 jitter = rng_next2(rng);
+            V2 lens = rng_next2(rng);
+            V3 o, d;
+            camera_ray(cam.c, float(x) + jitter.x, float(y) + jitter.y, w, h, lens, o, d);
+            wk.init(o, d, kInf, sl);
+            return pixel;
+        },
+        [&](uint32_t pixel, const W& wk, const float4& hh) {
+            out[pixel] = __float_as_int(hh.x) >= 0 ? make_float4(wk.tmax, hh.x, hh.y, hh.z) : make_float4(kInf, __int_as_float(-1), 0.0f, 0.0f);
+        });
+}
+
+__global__ void __launch_bounds__(128) k_occlusion_probe_pairs(const DevScene* sp, const float4* rays, int n, int4* out, uint32_t* claim,
+                                                              uint32_t visits) {
+    extern __shared__ int smem_stack[];
+    PairSlots& ps = reinterpret_cast<PairSlots*>(smem_stack + kSmemStack * blockDim.x)[threadIdx.x >> 5];
+    const DevScene& s = *sp;
+    const WalkScene uni{s.nodes, s.tris, sp};
+    TraversalCounters tc{0, 0, 0};
+    uint32_t warp_steps = 0, start = 0;
+    using W = PairWalker<true, true>;
+    walk_queue_pairs<W, kStackSize - kSmemStack, true, true, true>(
+        uint32_t(n), claim, 24u, visits, smem_stack + threadIdx.x, blockDim.x, ps, uni, tc, warp_steps,
+        [&](uint32_t i, W& wk, WalkScene&, const PairLane& sl) {
+            const float4 a = rays[2 * i], b = rays[2 * i + 1];
+            wk.init(xyz(a), xyz(b), a.w, sl);
+            start = tc.nodes;
+            return i;
+        },
+        [&](uint32_t i, const W&, const float4& hh) {
+            const int tri = __float_as_int(hh.x);
+            out[i] = make_int4(tri >= 0 ? 1 : 0, tri, int(tc.nodes - start), -1);
+        });
+}
+
 // The light pick of the first vertex of each pixel's sample (integrator.h:199-209).
 __global__ void __launch_bounds__(128) k_light_picks(const DevScene* sp, const DevView* vp, int4* out) {
     extern __shared__ int smem_stack[];
@@ -1511,9 +1564,17 @@ cudaError_t wf_accumulate(const DevView* d_view, const DevView& h_view, int firs
 }
 
 cudaError_t wf_trace_primary(const DevScene* scene, const float* cam16, int w, int h, uint32_t frame, uint32_t seed, float4* out,
-                             cudaStream_t stream) {
+                             uint32_t* claim, uint32_t pair_visits, cudaStream_t stream) {
     CameraArg c;
     for (int i = 0; i < 16; i++) c.c[i] = cam16[i];
+    if (pair_visits > 0) {
+        const size_t smem = size_t(kSmemStack) * 128 * sizeof(int) + 4 * sizeof(PairSlots);
+        const uint32_t n = uint32_t(w) * uint32_t(h), blocks = std::min<uint32_t>((n + 127) / 128, 148u * 16u);
+        cudaError_t e = cudaMemsetAsync(claim, 0, sizeof(uint32_t), stream);
+        if (e != cudaSuccess) return e;
+        k_trace_primary_pairs<<<blocks, 128, smem, stream>>>(scene, c, w, h, frame, seed, out, claim, pair_visits);
+        return cudaGetLastError();
+    }
     dim3 grid((w + 15) / 16, (h + 7) / 8);
     size_t smem = size_t(kSmemStack) * 128 * sizeof(int);
     k_trace_primary<<<grid, 128, smem, stream>>>(scene, c, w, h, frame, seed, out);
@@ -1527,8 +1588,17 @@ cudaError_t wf_light_picks(const DevScene* scene, const DevView* view, int4* out
     return cudaGetLastError();
 }
 
-cudaError_t wf_occlusion_probe(const DevScene* scene, const float4* rays, int n, int wide, int4* out, cudaStream_t stream) {
+cudaError_t wf_occlusion_probe(const DevScene* scene, const float4* rays, int n, int wide, int4* out, uint32_t* claim, uint32_t pair_visits,
+                               cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
+    if (pair_visits > 0 && !wide) {
+        const size_t smem = size_t(kSmemStack) * 128 * sizeof(int) + 4 * sizeof(PairSlots);
+        const uint32_t blocks = std::min<uint32_t>((uint32_t(n) + 127) / 128, 148u * 16u);
+        cudaError_t e = cudaMemsetAsync(claim, 0, sizeof(uint32_t), stream);
+        if (e != cudaSuccess) return e;
+        k_occlusion_probe_pairs<<<blocks, 128, smem, stream>>>(scene, rays, n, out, claim, pair_visits);
+        return cudaGetLastError();
+    }
     const size_t smem = size_t(kSmemStack) * 128 * sizeof(int);
     k_occlusion_probe<<<(n + 127) / 128, 128, smem, stream>>>(scene, rays, n, wide, out);
     return cudaGetLastError();

@@ -142,14 +142,16 @@ cudaError_t wf_accumulate(const DevView* d_view, const DevView& h_view, int firs
 // rgb[3i..3i+2] = accum[i].xyz * scale (or the plain xyz when apply_scale is false).
 cudaError_t wf_resolve(const float4* accum, uint32_t n, float scale, bool apply_scale, float* rgb, cudaStream_t stream);
 
-// Probes (same device functions as the wavefront).
+// Probes (same device functions as the wavefront). With pair_visits > 0 the walks are the pair walks
+// of the wavefront's default kernels, over a queue counted in `claim` (one device word).
 cudaError_t wf_trace_primary(const DevScene* scene, const float* cam16, int w, int h, uint32_t frame, uint32_t seed,
-                             float4* out, cudaStream_t stream);
+                             float4* out, uint32_t* claim, uint32_t pair_visits, cudaStream_t stream);
 cudaError_t wf_light_picks(const DevScene* scene, const DevView* view, int4* out, int w, int h, cudaStream_t stream);
 cudaError_t wf_heatmap(const DevScene* scene, const float* cam16, int w, int h, float* out, cudaStream_t stream);
 // Any-hit walks of n rays (2 float4 each: origin + tmax, direction + unused): out[i] = (occluded,
 // first accepted triangle or -1, node visits, triangle tests).
-cudaError_t wf_occlusion_probe(const DevScene* scene, const float4* rays, int n, int wide, int4* out, cudaStream_t stream);
+cudaError_t wf_occlusion_probe(const DevScene* scene, const float4* rays, int n, int wide, int4* out, uint32_t* claim, uint32_t pair_visits,
+                               cudaStream_t stream);
 
 struct DisplayParams {
     int w, h, mode;

@@ -26,14 +26,17 @@ def frame():
 
 
 def test_full_frame_primary_hits_equal_photons(frame):
+    """Both closest-hit walks: the pair walk of the default kernels and the per-lane walk."""
     g, b, ref = frame
     cam = g.camera(W / H)
+    theirs = ref.trace_primary(cam, W, H, 0, SEED)
     r = native.Renderer()
     r.upload(b.desc)
-    ours = r.trace_primary(cam, W, H, 0, SEED)
+    for pair_walk in (5, 0):
+        r.set_tuning(pair_walk=pair_walk)
+        ours = r.trace_primary(cam, W, H, 0, SEED)
+        assert np.array_equal(ours.view(np.uint32), theirs.view(np.uint32)), f"pair_walk={pair_walk}"
     r.close()
-    theirs = ref.trace_primary(cam, W, H, 0, SEED)
-    assert np.array_equal(ours.view(np.uint32), theirs.view(np.uint32))
     assert (O.hits_tri(ours) >= 0).mean() > 0.3
 
 

@@ -330,18 +330,28 @@ def test_ray_sorting_is_bit_identical(bits):
         assert np.array_equal(imgs[0].view(np.uint32), img.view(np.uint32))
 
 
+@pytest.mark.parametrize("pair_walk", [0, 5])
 @pytest.mark.parametrize("name", ["terrain", "materials", "box"])
-def test_any_hit_walk_bit_exact(renderer, name):
+def test_any_hit_walk_bit_exact(renderer, name, pair_walk):
     """The shadow rays' any-hit walk on the device, directly: on random rays (half of them with a
-    finite tmax), whether each is occluded, the triangle its walk accepts first and its node visits and
-    triangle tests equal the oracle's (the terrain has alpha-masked materials, so the alpha test is in
-    the walk). The 4-wide walk gives the same answers."""
+    finite tmax), whether each is occluded, the triangle its walk accepts first and its node visits (and
+    for the per-lane walk its triangle tests; a pair walk's tests are done by other lanes) equal the
+    oracle's (the terrain has alpha-masked materials, so the alpha test is in the walk), for the pair
+    walk of the default kernels and the per-lane walk. The 4-wide walk gives the same answers."""
     desc, camf, keep = scenes.scene(name)
     renderer.upload(desc)
+    before = renderer.tuning()["pair_walk"]
+    renderer.set_tuning(pair_walk=pair_walk)
     rays = scenes.random_rays(desc, 50000, seed=7)
-    got = renderer.occlusion_probe(rays)
+    try:
+        got = renderer.occlusion_probe(rays)
+    finally:
+        renderer.set_tuning(pair_walk=before)  # the module's renderer is shared
     want = O.orc_occluded(desc, rays)
-    assert np.array_equal(got, want)
+    if pair_walk:
+        assert np.array_equal(got[:, :3], want[:, :3]) and (got[:, 3] == -1).all()
+    else:
+        assert np.array_equal(got, want)
     wide = renderer.occlusion_probe(rays, wide=True)
     assert np.array_equal(wide[:, 0], want[:, 0])
     assert 0.2 < got[:, 0].mean() < 0.95
