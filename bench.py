@@ -312,7 +312,7 @@ def systems_sections(r, g, desc, rank):
         built.append(gs.build(gpu=k >= 2) if k != 1 else None)
     descs = [built[0].desc, desc, built[2].desc, built[3].desc]
     budget = 150 << 30
-    server = native.Server(budget_bytes=budget)
+    server = native.Server(budget_bytes=budget, device=r_device(r))
     sids = [server.add_scene(d) for d in descs]
     pairs = list(zip(sids, descs))
     stream = workloads.request_stream(pairs, SERVED_REQUESTS, SERVED_RATE, seed=7)
@@ -341,7 +341,7 @@ def systems_sections(r, g, desc, rank):
                      "served_over_plain": served["msamples_per_s"] / plain["msamples_per_s"]}
     # Eight real-time SVGF sessions served by the same server alongside the same stream (the server's
     # session lane), and the same sessions on renderers of their own.
-    server = native.Server(budget_bytes=budget)
+    server = native.Server(budget_bytes=budget, device=r_device(r))
     sids = [server.add_scene(d) for d in descs]
     serving.run_served(server, warm)
     both = serving.run_sessions_served(server, sids[1], desc, 8, 120, 1600, 900,
@@ -351,7 +351,7 @@ def systems_sections(r, g, desc, rank):
     out["sessions"] = dict(both, workload="8 real-time SVGF sessions (120-frame orbits, 0.5 deg/frame, of the 262K scene, 1600x900, "
                                           "1 spp) served by the request server alongside the served stream above",
                            api="pt_server_open_session / pt_server_submit_frame",
-                           standalone=dict(sessions.run_sessions(desc, 8, 120, 1600, 900), api="pt_render_denoised, one renderer per session"))
+                           standalone=dict(sessions.run_sessions(desc, 8, 120, 1600, 900, device=r_device(r)), api="pt_render_denoised, one renderer per session"))
     return out
 
 
@@ -508,7 +508,8 @@ def main():
             mk["wavefront_over_megakernel"] = value / mk["msamples_per_s"]
             mk["wavefront_e2e_over_megakernel"] = e2e_value / mk["msamples_per_s"]
         line["megakernel"] = mk
-    if not args.no_systems:
+    if world == 1 and not args.no_systems:
+        # The batched, served and session forms are single-GPU forms; a replica run reports the frame.
         line.update(systems_sections(r, g, desc, rank))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(desc, cam)
