@@ -238,8 +238,8 @@ __device__ __forceinline__ void walk_queue(uint32_t n, uint32_t* claim, uint32_t
 }
 
 // ---- the pair walk -----------------------------------------------------------------------------------
-// A warp's shared memory in the pair walk (2,048 bytes after the block's stacks): each lane's PairLane
-// slots and the owners' result slots of a pair pass.
+// A warp's shared memory in the pair walk (2,080 bytes after the block's stacks): each lane's PairLane
+// slots, the owners' result slots of a pair pass and a round's owner table.
 struct PairSlots {
     float4 ray[32];
     int4 leaves[32];
@@ -258,9 +258,9 @@ static_assert(sizeof(PairSlots) == 2080, "PairSlots layout");
 // by five dependent shuffles: trace 23.8 -> 23.55, shadow 10.92 -> 10.85 ms per 1080p frame),
 // takes its origin by shuffles and its direction, tmax and leaf ranges from its slots (`scene`: the
 // lane's own scene, in multi-scene launches), tests that triangle against the owner's tmax, and an
-// accepted pair enters the owner's slot by a
-// 64-bit atomicMin of (distance bits << 32 | pair index): positive distances order as their bits, so
-// the owner gets its least distance, on a tie its earliest pair. A sequential leaf walk (traverse.h
+// accepted pair enters the owner's slot by a 64-bit atomicMin of (distance bits << 32 | pair index):
+// positive distances order as their bits, so the owner gets its least distance, on a tie its earliest
+// pair. A sequential leaf walk (traverse.h
 // :93-104) accepts a triangle only when it lowers tmax, so it ends on the first pair of least distance
 // below the entering tmax: the same triangle, distance and barycentrics. Any-hit keys are the pair
 // index alone (the first accepted pair, where the sequential walk stops). An owner whose pairs span two
