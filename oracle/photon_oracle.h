@@ -3,7 +3,7 @@
  *
  * A plain-C restatement of Photon's path-tracing hot path (render_sample → trace_path with BVH2
  * traversal, the glTF BSDF, NEE + MIS light sampling, Russian roulette) and of its SVGF denoiser, on
- * the scene arrays of include/photon_wavefront.h. It is the checker the CUDA path is compared with.
+ * the scene arrays of include/photon_wavefront.h. It is the oracle the CUDA path is compared with.
  * Every function cites the Photon source it restates (paths relative to the Photon repository).
  *
  * Pinning: tests/test_oracle_pinning.py checks this restatement bit-for-bit against Photon's own CPU

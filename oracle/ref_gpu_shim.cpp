@@ -1,7 +1,7 @@
 // Test-infrastructure shim over Photon's CUDA code: the one-thread-per-pixel megakernel renderer
 // (src/render/gpu_renderer.cu) and the SVGF denoiser (src/denoise/svgf.cu), built unchanged with
 // Photon's own flags by oracle/Makefile into oracle/_ref/libphoton_ref_gpu.so. Used only as the SVGF
-// checker (identical G-buffers in, outputs compared) and as the megakernel comparison.
+// oracle (identical G-buffers in, outputs compared) and as the megakernel comparison.
 #include <cstring>
 #include <string>
 #include <vector>

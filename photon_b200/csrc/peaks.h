@@ -1,4 +1,4 @@
-// Bandwidth probes for the roofline denominators that no driver-measured figure covers.
+// Bandwidth probes for the roofline denominators that the measured-peaks file does not cover.
 #pragma once
 
 #include <cstddef>

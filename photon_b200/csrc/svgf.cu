@@ -607,7 +607,7 @@ void SvgfDenoiser::resize(int w, int h) {
     h_ = h;
     has_history_ = false;
     // Tensor maps of the TMA a-trous passes over edge_, filter_[0], filter_[1]; without them (no
-    // encoder in the driver, or a shape it rejects) the passes read global memory directly.
+    // encoder in the CUDA driver, or a shape it rejects) the passes read global memory directly.
     build_tma_plan();
 }
 
