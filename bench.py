@@ -101,7 +101,9 @@ def barrier(dist):
 
 
 class ClockSampler:
-    """nvidia-smi samples (every 200 ms) of SM clock and throttle reasons during the timed region."""
+    """nvidia-smi samples (every 100 ms) of SM clock and throttle reasons during the timed region; start()
+    returns once the first sample is in (nvidia-smi takes a moment to come up), so the samples cover the
+    region from its start."""
 
     FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
@@ -114,12 +116,16 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        deadline = time.time() + 5.0
+        while not self.lines and self.proc.poll() is None and time.time() < deadline:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -363,7 +369,7 @@ def r_device(r):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
