@@ -39,6 +39,9 @@ WORKLOAD = "262,144-triangle terrain scene (value-noise height field + 200 insta
            "64 emitters, 4 punctual lights, 1024x512 HDR sky), 1920x1080, 16 spp, max depth 12, seed 1"
 # Algorithmic bytes of the traversal kernels: one 64-byte node per visit, one 48-byte triangle per test.
 NODE_BYTES, TRI_BYTES = 64, 48
+# Modelled bytes of one shaded vertex in k_shade (path state in and out, hit, shadow entry, triangle,
+# indices, vertex attributes, material).
+SHADE_BYTES_PER_VERTEX = 450
 # DRAM bytes (read + write) per traced ray of the closest-hit walk: its first launch in the 960x540x4
 # profile case of the same scene (photon_b200/profile_case.py; 2,073,600 camera rays, 75.03 MB read +
 # 11.30 MB written in one ncu capture), scaled by the rays of a launch here: mostly the path state
@@ -461,6 +464,10 @@ def main():
     trace_launches = max(1, prof.trace.launches)
     achieved = (trace_bytes_per_frame * args.steps) / (prof.trace.ms / 1000.0) / 1e9 if prof.trace.ms > 0 else 0.0
     shadow_achieved = (shadow_bytes_per_frame * args.steps) / (prof.shadow.ms / 1000.0) / 1e9 if prof.shadow.ms > 0 else 0.0
+    # Every traced closest-hit ray of a queued iteration is one shaded vertex (the tail's are counted in
+    # closest_rays too, so this slightly overstates the shade kernel's share of them).
+    shaded_vertices = counts.closest_rays
+    shade_achieved = (shaded_vertices * SHADE_BYTES_PER_VERTEX * args.steps) / (prof.shade.ms / 1000.0) / 1e9 if prof.shade.ms > 0 else 0.0
     # The scene (nodes, triangles) stays in the 126 MB L2 during a frame, so the walk's bytes are L2
     # (and L1) traffic: the live L2 read probe is the bandwidth they are bounded by. The HBM fraction
     # is kept beside it because the copy bandwidth is the measured peak of the schema.
@@ -491,7 +498,15 @@ def main():
                 "shadow": {"kernel": "k_shadow_pairs (any-hit BVH traversal, pair walk)" if pairs else "k_shadow (any-hit BVH traversal)",
                            "bytes_per_frame": shadow_bytes_per_frame,
                            "ms_per_frame": prof.shadow.ms / args.steps, "achieved": shadow_achieved,
-                           "l2_frac": shadow_achieved / l2_peak if l2_peak > 0 else None, "hbm_frac": shadow_achieved / peak}}
+                           "l2_frac": shadow_achieved / l2_peak if l2_peak > 0 else None, "hbm_frac": shadow_achieved / peak},
+                "shade": {"kernel": "k_shade (material-sorted shading of the traced paths)",
+                          "model": f"{SHADE_BYTES_PER_VERTEX} B per shaded vertex: path state 80 B in and out, hit 16 B, "
+                                   "shadow entry 48 B, triangle record, vertex indices, three vertices' attributes and "
+                                   "the material (a model, not a count)",
+                          "vertices_per_frame": shaded_vertices,
+                          "ms_per_frame": prof.shade.ms / args.steps, "achieved": shade_achieved,
+                          "hbm_frac": shade_achieved / peak,
+                          "limiter": "latency: attribute, material and texture gathers at 16 warps per SM (114 registers)"}}
     rays_per_sample = (counts.closest_rays + counts.shadow_rays) / samples_per_step
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

@@ -269,10 +269,13 @@ typedef struct pt_tuning {
 } pt_tuning;
 int32_t pt_set_tuning(pt_renderer* r, const pt_tuning* t);
 int32_t pt_get_tuning(const pt_renderer* r, pt_tuning* t);
-/* The autotuner: picks path capacity, block shapes, material sorting, graph cadence, ray sorting and the tail size for the uploaded
- * scene by coordinate descent, timing probe renders of `camera` (at most `probe_samples` paths each,
- * into private buffers: the accumulation is untouched). Applies the best tuning, returns it in
- * `chosen` (optional) and the probe throughput of the default and chosen tunings (samples/s). */
+/* The autotuner: picks path capacity, block shapes, material sorting, graph cadence, ray sorting, the
+ * tail size and the walk knobs (4-wide shadows, refill thresholds, burst, shadow order, pair walks) for
+ * the uploaded scene by coordinate descent, timing probe renders of `camera` (at most `probe_samples`
+ * paths each, into private buffers: the accumulation is untouched). A knob moves for a gain above 2%,
+ * and the final pick is kept only if it still beats the starting tuning by 2% when both are timed
+ * again. Applies the kept tuning, returns it in `chosen` (optional) and the probe throughput of the
+ * starting and kept tunings (samples/s). */
 int32_t pt_autotune(pt_renderer* r, const pt_camera* camera, const pt_render_settings* settings, int32_t spp,
                     uint64_t probe_samples, pt_tuning* chosen, double* default_rate, double* tuned_rate);
 

@@ -794,7 +794,7 @@ void Renderer::get_tuning(pt_tuning* t) const {
 
 // Coordinate descent over the knobs, one at a time, each candidate timed on the same probe view set.
 // Every probe runs twice and keeps the faster time, after a warm-up render with the candidate (graph
-// capture and buffer growth are not timed). A knob moves only for a gain above 1%. The probe renders
+// capture and buffer growth are not timed). A knob moves only for a gain above 2%. The probe renders
 // into the batched-view buffers, whose previous contents are put back afterwards.
 void Renderer::tune_on(const std::vector<pt_view>& probe, pt_tuning* chosen, double* default_rate, double* tuned_rate) {
     uint64_t samples = 0;
@@ -823,6 +823,7 @@ void Renderer::tune_on(const std::vector<pt_view>& probe, pt_tuning* chosen, dou
         Tuning base = engine_->tuning();
         engine_->set_tuning(base);
         double best_rate = time_probe();
+        const double base_rate = best_rate;
         if (default_rate) *default_rate = best_rate;
         Tuning best = base;
         auto try_knob = [&](auto setter, std::initializer_list<int> values) {
@@ -860,7 +861,7 @@ void Renderer::tune_on(const std::vector<pt_view>& probe, pt_tuning* chosen, dou
         const double best_again = time_probe();
         if (!(best_again > base_again * 1.02)) {
             best = base;
-            best_rate = std::max(base_again, best_rate);
+            best_rate = std::max(base_again, base_rate);  // the kept record's rate: its faster timing
             engine_->set_tuning(base);
         }
         if (tuned_rate) *tuned_rate = best_rate;
